@@ -1,0 +1,291 @@
+"""Python binding of libhpm_cuda.so (the C ABI in include/hpm_capi.h).
+
+This is the test/bench harness view of the B200 HPM-MVS++ hot path.  It mirrors
+the C ABI one to one; the product logic lives in the CUDA library.  There is no
+CPU fallback: constructing a Context without the built library or without a CUDA
+device raises.
+
+The directory name contains a hyphen, so load it with `load_package()` of
+__graft_entry__.py or importlib (tests/conftest.py registers it as `hpm_b200`).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "_build", "libhpm_cuda.so")
+
+# ---- ABI mirror of include/hpm_types.h -------------------------------------------------
+
+MODE_GEOM = 1 << 0
+MODE_PRIOR = 1 << 1
+MODE_MULTIGEOM = 1 << 2
+MODE_HIERARCHY = 1 << 3
+MODE_UPSAMPLE = 1 << 4
+MODE_MAND = 1 << 5
+
+MAP_DEPTH = 0
+MAP_DEPTH_GEOM = 1
+MAP_NORMAL = 2
+MAP_COST = 3
+MAP_CONF = 4
+MAP_TEXTURE0 = 8
+
+EXPORTED_SYMBOLS = (
+    "hpm_create", "hpm_destroy", "hpm_last_error", "hpm_set_view", "hpm_set_map", "hpm_get_map",
+    "hpm_set_canny", "hpm_set_prior", "hpm_run_patchmatch", "hpm_eval_costs", "hpm_set_address_mode",
+    "hpm_launch_count", "hpm_synchronize", "hpm_sample_view", "hpm_debug_run_partial",
+)
+
+
+class Camera(ctypes.Structure):
+    """hpm_camera == struct Camera of the reference (main.h:39-47), 100 bytes."""
+
+    _fields_ = [
+        ("K", ctypes.c_float * 9),
+        ("R", ctypes.c_float * 9),
+        ("t", ctypes.c_float * 3),
+        ("height", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("depth_min", ctypes.c_float),
+        ("depth_max", ctypes.c_float),
+    ]
+
+    @classmethod
+    def make(cls, K, R, t, width, height, depth_min, depth_max) -> "Camera":
+        c = cls()
+        c.K[:] = [float(v) for v in np.asarray(K, np.float32).ravel()]
+        c.R[:] = [float(v) for v in np.asarray(R, np.float32).ravel()]
+        c.t[:] = [float(v) for v in np.asarray(t, np.float32).ravel()]
+        c.width, c.height = int(width), int(height)
+        c.depth_min, c.depth_max = float(depth_min), float(depth_max)
+        return c
+
+    def copy(self) -> "Camera":
+        c = Camera()
+        ctypes.memmove(ctypes.byref(c), ctypes.byref(self), ctypes.sizeof(Camera))
+        return c
+
+    def scaled(self, width: int, height: int, orig_width: int, orig_height: int) -> "Camera":
+        """K rescaled to a resized image (HPM.cpp:669-676, float32 arithmetic)."""
+        c = self.copy()
+        sx = np.float32(width) / np.float32(orig_width)
+        sy = np.float32(height) / np.float32(orig_height)
+        c.K[0] = float(np.float32(c.K[0]) * sx)
+        c.K[2] = float(np.float32(c.K[2]) * sx)
+        c.K[4] = float(np.float32(c.K[4]) * sy)
+        c.K[5] = float(np.float32(c.K[5]) * sy)
+        c.width, c.height = int(width), int(height)
+        return c
+
+
+class Params(ctypes.Structure):
+    """hpm_params (PatchMatchParams, HPM.h:229-252)."""
+
+    _fields_ = [
+        ("max_iterations", ctypes.c_int32),
+        ("patch_size", ctypes.c_int32),
+        ("num_images", ctypes.c_int32),
+        ("radius_increment", ctypes.c_int32),
+        ("sigma_spatial", ctypes.c_float),
+        ("sigma_color", ctypes.c_float),
+        ("top_k", ctypes.c_int32),
+        ("depth_min", ctypes.c_float),
+        ("depth_max", ctypes.c_float),
+        ("scaled_cols", ctypes.c_int32),
+        ("scaled_rows", ctypes.c_int32),
+        ("mode", ctypes.c_uint32),
+    ]
+
+    @classmethod
+    def make(cls, num_images: int, depth_min: float, depth_max: float, mode: int = 0) -> "Params":
+        p = cls()
+        p.max_iterations = 3  # RunPatchMatch hard-codes 3 iterations (HPM.cu:3013)
+        p.patch_size = 11
+        p.num_images = num_images
+        p.radius_increment = 2
+        p.sigma_spatial = 5.0
+        p.sigma_color = 3.0
+        p.top_k = 4
+        p.depth_min = depth_min
+        p.depth_max = depth_max
+        p.scaled_cols = 0
+        p.scaled_rows = 0
+        p.mode = mode
+        return p
+
+
+def widened_range(cam: Camera) -> tuple[float, float]:
+    """params.depth_min/max = 0.6 / 1.2 x the camera range (HPM.cpp:685-686)."""
+    return float(np.float32(cam.depth_min) * np.float32(0.6)), float(np.float32(cam.depth_max) * np.float32(1.2))
+
+
+class HPMError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise HPMError(f"libhpm_cuda.so is not built ({path}); run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    vp, i32, f = ctypes.c_void_p, ctypes.c_int32, ctypes.c_float
+    lib.hpm_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+    lib.hpm_destroy.argtypes = [vp]
+    lib.hpm_destroy.restype = None
+    lib.hpm_last_error.argtypes = [vp]
+    lib.hpm_last_error.restype = ctypes.c_char_p
+    lib.hpm_set_view.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Camera)]
+    lib.hpm_set_map.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int]
+    lib.hpm_get_map.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_size_t,
+                                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    lib.hpm_set_canny.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int]
+    lib.hpm_set_prior.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int]
+    lib.hpm_run_patchmatch.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int,
+                                       ctypes.c_uint64]
+    lib.hpm_eval_costs.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int, vp, vp,
+                                   vp]
+    lib.hpm_set_address_mode.argtypes = [vp, ctypes.c_int]
+    lib.hpm_launch_count.argtypes = [vp]
+    lib.hpm_launch_count.restype = ctypes.c_int64
+    lib.hpm_synchronize.argtypes = [vp]
+    lib.hpm_sample_view.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
+    lib.hpm_debug_run_partial.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int,
+                                          ctypes.c_uint64, ctypes.c_int, vp, vp, vp, vp]
+    for name in EXPORTED_SYMBOLS:
+        getattr(lib, name)
+    del i32, f
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """One hpm_ctx: resident views and maps on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.hpm_create(device, ctypes.byref(h))
+        if rc != 0 or not h.value:
+            raise HPMError(f"hpm_create(device={device}) failed with status {rc} (no CUDA device?)")
+        self.h = h
+        self.views: dict[int, tuple[int, int]] = {}
+
+    def close(self) -> None:
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.hpm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc != 0:
+            msg = self.lib.hpm_last_error(self.h)
+            raise HPMError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+    def set_address_mode(self, mode: int) -> None:
+        self._check(self.lib.hpm_set_address_mode(self.h, mode), "hpm_set_address_mode")
+
+    def set_view(self, view: int, gray: np.ndarray, cam: Camera) -> None:
+        g = np.ascontiguousarray(gray, dtype=np.float32)
+        h, w = g.shape
+        self._check(self.lib.hpm_set_view(self.h, view, _ptr(g), w, h, ctypes.byref(cam)), "hpm_set_view")
+        self.views[view] = (w, h)
+
+    def set_map(self, view: int, kind: int, data: np.ndarray) -> None:
+        d = np.ascontiguousarray(data, dtype=np.float32)
+        h, w = d.shape[:2]
+        self._check(self.lib.hpm_set_map(self.h, view, kind, _ptr(d), w, h), "hpm_set_map")
+
+    def get_map(self, view: int, kind: int) -> np.ndarray:
+        w, h = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.hpm_get_map(self.h, view, kind, None, 0, ctypes.byref(w), ctypes.byref(h)), "hpm_get_map")
+        ch = 3 if kind == MAP_NORMAL else 1
+        out = np.empty((h.value, w.value, ch) if ch > 1 else (h.value, w.value), np.float32)
+        self._check(self.lib.hpm_get_map(self.h, view, kind, _ptr(out), out.size, None, None), "hpm_get_map")
+        return out
+
+    def set_canny(self, view: int, edges: np.ndarray) -> None:
+        e = np.ascontiguousarray(edges, dtype=np.uint8)
+        h, w = e.shape
+        self._check(self.lib.hpm_set_canny(self.h, view, _ptr(e), w, h), "hpm_set_canny")
+
+    def set_prior(self, view: int, planes: np.ndarray, mask: np.ndarray) -> None:
+        p = np.ascontiguousarray(planes, dtype=np.float32)
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        h, w = m.shape
+        self._check(self.lib.hpm_set_prior(self.h, view, _ptr(p), _ptr(m), w, h), "hpm_set_prior")
+
+    def run_patchmatch(self, ref: int, srcs: Sequence[int], params: Params, texture_level: int = 0,
+                       seed: int = 0) -> None:
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        self._check(self.lib.hpm_run_patchmatch(self.h, ref, _ptr(s), len(s), ctypes.byref(params), texture_level,
+                                                ctypes.c_uint64(seed)), "hpm_run_patchmatch")
+
+    def eval_costs(self, ref: int, srcs: Sequence[int], params: Params, px: np.ndarray,
+                   planes: np.ndarray) -> np.ndarray:
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        p = np.ascontiguousarray(px, dtype=np.int32).reshape(-1, 2)
+        pl = np.ascontiguousarray(planes, dtype=np.float32).reshape(-1, 4)
+        out = np.empty((p.shape[0], len(s)), np.float32)
+        self._check(self.lib.hpm_eval_costs(self.h, ref, _ptr(s), len(s), ctypes.byref(params), p.shape[0], _ptr(p),
+                                            _ptr(pl), _ptr(out)), "hpm_eval_costs")
+        return out
+
+    def sample_view(self, view: int, xy: np.ndarray) -> np.ndarray:
+        c = np.ascontiguousarray(xy, dtype=np.float32).reshape(-1, 2)
+        out = np.empty(c.shape[0], np.float32)
+        self._check(self.lib.hpm_sample_view(self.h, view, c.shape[0], _ptr(c), _ptr(out)), "hpm_sample_view")
+        return out
+
+    def run_partial(self, ref: int, srcs: Sequence[int], params: Params, n_half_sweeps: int, texture_level: int = 0,
+                    seed: int = 0) -> dict:
+        """Init + n half-sweeps; returns the raw run state (camera-frame planes)."""
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        w, h = self.views[ref]
+        planes = np.empty((h, w, 4), np.float32)
+        costs = np.empty((h, w), np.float32)
+        sel = np.empty((h, w), np.uint32)
+        draws = np.empty((h, w), np.uint32)
+        self._check(self.lib.hpm_debug_run_partial(self.h, ref, _ptr(s), len(s), ctypes.byref(params), texture_level,
+                                                   ctypes.c_uint64(seed), n_half_sweeps, _ptr(planes), _ptr(costs),
+                                                   _ptr(sel), _ptr(draws)), "hpm_debug_run_partial")
+        return {"planes": planes, "costs": costs, "selected_views": sel, "rng_draw": draws}
+
+    def synchronize(self) -> None:
+        self._check(self.lib.hpm_synchronize(self.h), "hpm_synchronize")
+
+    def launch_count(self) -> int:
+        return int(self.lib.hpm_launch_count(self.h))
+
+
+@dataclass
+class View:
+    """One view of a scene at some resolution."""
+
+    gray: np.ndarray  # float32 H x W
+    cam: Camera

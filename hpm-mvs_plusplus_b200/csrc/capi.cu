@@ -1,0 +1,294 @@
+// C ABI implementation: a context owns every view's grey image (as a
+// linear-filtered texture), its resident "dmb" maps and the work buffers of a
+// PatchMatch run.  See include/hpm_capi.h for the contract.
+#include "hpm_capi.h"
+#include "ctx.hpp"
+#include "pm_kernels.cuh"
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+using namespace hpm;
+
+namespace hpm {
+
+int Ctx::fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    err = buf;
+    return code;
+}
+
+int Ctx::cuda_fail(cudaError_t e, const char* what) {
+    return fail(HPM_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+template <class T>
+static cudaError_t ensure(T*& p, size_t& cap, size_t n) {
+    if (n <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc((void**)&p, std::max<size_t>(n, 1) * sizeof(T));
+    if (e == cudaSuccess) cap = n;
+    return e;
+}
+
+cudaError_t Ctx::ensure_map(int view, int kind, int w, int h) {
+    DevMap& m = views[view].maps[kind];
+    const int ch = (kind == HPM_MAP_NORMAL) ? 3 : 1;
+    cudaError_t e = ensure(m.ptr, m.cap, (size_t)w * h * ch);
+    if (e == cudaSuccess) { m.w = w; m.h = h; m.ch = ch; }
+    return e;
+}
+
+cudaError_t Ctx::ensure_run(size_t n) {
+    cudaError_t e;
+    if ((e = ensure(planes, run_cap_planes, n)) != cudaSuccess) return e;
+    if ((e = ensure(costs, run_cap_costs, n)) != cudaSuccess) return e;
+    if ((e = ensure(pre_costs, run_cap_pre, n)) != cudaSuccess) return e;
+    if ((e = ensure(sel, run_cap_sel, n)) != cudaSuccess) return e;
+    if ((e = ensure(rng, run_cap_rng, n)) != cudaSuccess) return e;
+    if ((e = ensure(conf, run_cap_conf, n)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+Ctx::~Ctx() {
+    for (auto& v : views) {
+        if (v.tex) cudaDestroyTextureObject(v.tex);
+        if (v.arr) cudaFreeArray(v.arr);
+        if (v.gray) cudaFree(v.gray);
+        for (auto& m : v.maps) if (m.ptr) cudaFree(m.ptr);
+        if (v.canny) cudaFree(v.canny);
+        if (v.prior) cudaFree(v.prior);
+        if (v.pmask) cudaFree(v.pmask);
+    }
+    for (void* p : { (void*)planes, (void*)costs, (void*)pre_costs, (void*)sel, (void*)rng, (void*)conf,
+                     (void*)scaled, (void*)scratch })
+        if (p) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+// Relative pose of ComputeHomography (HPM.cu:251-279), evaluated on the host
+// in float with the reference's operation order.
+void compute_pose(const hpm_camera& rc, const hpm_camera& sc, ViewPoseH& vp) {
+    float rC[3], sC[3], Cr[3];
+    rC[0] = -(rc.R[0] * rc.t[0] + rc.R[3] * rc.t[1] + rc.R[6] * rc.t[2]);
+    rC[1] = -(rc.R[1] * rc.t[0] + rc.R[4] * rc.t[1] + rc.R[7] * rc.t[2]);
+    rC[2] = -(rc.R[2] * rc.t[0] + rc.R[5] * rc.t[1] + rc.R[8] * rc.t[2]);
+    sC[0] = -(sc.R[0] * sc.t[0] + sc.R[3] * sc.t[1] + sc.R[6] * sc.t[2]);
+    sC[1] = -(sc.R[1] * sc.t[0] + sc.R[4] * sc.t[1] + sc.R[7] * sc.t[2]);
+    sC[2] = -(sc.R[2] * sc.t[0] + sc.R[5] * sc.t[1] + sc.R[8] * sc.t[2]);
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 3; ++k)
+            vp.Rr[3 * r + k] = sc.R[3 * r] * rc.R[3 * k] + sc.R[3 * r + 1] * rc.R[3 * k + 1] + sc.R[3 * r + 2] * rc.R[3 * k + 2];
+    Cr[0] = rC[0] - sC[0]; Cr[1] = rC[1] - sC[1]; Cr[2] = rC[2] - sC[2];
+    for (int r = 0; r < 3; ++r) vp.tr[r] = sc.R[3 * r] * Cr[0] + sc.R[3 * r + 1] * Cr[1] + sc.R[3 * r + 2] * Cr[2];
+}
+
+// ---------------------------------------------------------------- small kernels
+
+__global__ void k_pack_planes(const float* __restrict__ normal, const float* __restrict__ depth,
+                              float4* __restrict__ planes, const float* __restrict__ cost_in,
+                              float* __restrict__ cost_out, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p;
+    p.x = normal ? normal[3 * (size_t)i] : 0.0f;
+    p.y = normal ? normal[3 * (size_t)i + 1] : 0.0f;
+    p.z = normal ? normal[3 * (size_t)i + 2] : 0.0f;
+    p.w = depth[i];
+    planes[i] = p;
+    if (cost_out) cost_out[i] = cost_in[i];
+}
+
+// Hierarchy input map (HPM.cpp:877-892): coarse normals with the coarse cost
+// (upsample) or the depth as w.
+__global__ void k_pack_scaled(const float* __restrict__ normal, const float* __restrict__ w_src,
+                              float4* __restrict__ out, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = make_float4(normal[3 * (size_t)i], normal[3 * (size_t)i + 1], normal[3 * (size_t)i + 2], w_src[i]);
+}
+
+__global__ void k_unpack_planes(const float4* __restrict__ planes, float* __restrict__ depth,
+                                float* __restrict__ normal, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = planes[i];
+    depth[i] = p.w;
+    normal[3 * (size_t)i] = p.x;
+    normal[3 * (size_t)i + 1] = p.y;
+    normal[3 * (size_t)i + 2] = p.z;
+}
+
+}  // namespace hpm
+
+// ---------------------------------------------------------------- C ABI
+
+extern "C" {
+
+int hpm_create(int device, hpm_ctx** out) {
+    if (!out) return HPM_E_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return HPM_E_CUDA;
+    if (cudaSetDevice(device) != cudaSuccess) return HPM_E_CUDA;
+    Ctx* c = new (std::nothrow) Ctx();
+    if (!c) return HPM_E_NOMEM;
+    c->device = device;
+    c->views.resize(HPM_MAX_VIEWS);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return HPM_E_CUDA;
+    }
+    *out = reinterpret_cast<hpm_ctx*>(c);
+    return HPM_OK;
+}
+
+void hpm_destroy(hpm_ctx* ctx) {
+    if (!ctx) return;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    delete c;
+}
+
+const char* hpm_last_error(const hpm_ctx* ctx) {
+    if (!ctx) return "null context";
+    return reinterpret_cast<const Ctx*>(ctx)->err.c_str();
+}
+
+int hpm_set_address_mode(hpm_ctx* ctx, int mode) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (mode != 0 && mode != 1) return c->fail(HPM_E_INVALID, "address mode must be 0 (clamp) or 1 (wrap)");
+    c->addr_mode = mode;
+    return HPM_OK;
+}
+
+int64_t hpm_launch_count(const hpm_ctx* ctx) { return ctx ? reinterpret_cast<const Ctx*>(ctx)->launches : 0; }
+
+int hpm_synchronize(hpm_ctx* ctx) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "synchronize");
+    return HPM_OK;
+}
+
+int hpm_set_view(hpm_ctx* ctx, int view, const float* gray, int w, int h, const hpm_camera* cam) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || !gray || !cam || w <= 0 || h <= 0)
+        return c->fail(HPM_E_INVALID, "hpm_set_view: bad arguments");
+    cudaSetDevice(c->device);
+    ViewState& v = c->views[view];
+    cudaError_t e = ensure(v.gray, v.gray_cap, (size_t)w * h);
+    if (e != cudaSuccess) return c->cuda_fail(e, "alloc grey image");
+    e = cudaMemcpyAsync(v.gray, gray, sizeof(float) * w * h, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "upload grey image");
+    v.w = w; v.h = h; v.cam = *cam;
+    v.cam.width = w; v.cam.height = h;
+    return c->bind_texture(view);
+}
+
+int hpm_set_map(hpm_ctx* ctx, int view, int kind, const float* data, int w, int h) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || kind < 0 || kind >= kNumMaps || !data || w <= 0 || h <= 0)
+        return c->fail(HPM_E_INVALID, "hpm_set_map: bad arguments");
+    cudaSetDevice(c->device);
+    cudaError_t e = c->ensure_map(view, kind, w, h);
+    if (e != cudaSuccess) return c->cuda_fail(e, "alloc map");
+    const DevMap& m = c->views[view].maps[kind];
+    e = cudaMemcpyAsync(m.ptr, data, sizeof(float) * (size_t)w * h * m.ch, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "upload map");
+    return HPM_OK;
+}
+
+int hpm_get_map(hpm_ctx* ctx, int view, int kind, float* data, size_t capacity, int* w, int* h) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || kind < 0 || kind >= kNumMaps)
+        return c->fail(HPM_E_INVALID, "hpm_get_map: bad arguments");
+    const DevMap& m = c->views[view].maps[kind];
+    if (!m.ptr || m.w == 0) return c->fail(HPM_E_STATE, "view %d has no map %d", view, kind);
+    if (w) *w = m.w;
+    if (h) *h = m.h;
+    const size_t n = (size_t)m.w * m.h * m.ch;
+    if (!data) return HPM_OK;
+    if (capacity < n) return c->fail(HPM_E_INVALID, "hpm_get_map: capacity %zu < %zu", capacity, n);
+    cudaSetDevice(c->device);
+    cudaError_t e = cudaMemcpyAsync(data, m.ptr, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "download map");
+    return HPM_OK;
+}
+
+int hpm_set_canny(hpm_ctx* ctx, int view, const uint8_t* edges, int w, int h) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || !edges || w <= 0 || h <= 0)
+        return c->fail(HPM_E_INVALID, "hpm_set_canny: bad arguments");
+    cudaSetDevice(c->device);
+    ViewState& v = c->views[view];
+    cudaError_t e = ensure(v.canny, v.canny_cap, (size_t)w * h);
+    if (e != cudaSuccess) return c->cuda_fail(e, "alloc canny");
+    e = cudaMemcpyAsync(v.canny, edges, (size_t)w * h, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "upload canny");
+    v.canny_w = w; v.canny_h = h;
+    return HPM_OK;
+}
+
+int hpm_set_prior(hpm_ctx* ctx, int view, const float* planes, const uint8_t* mask, int w, int h) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || !planes || !mask || w <= 0 || h <= 0)
+        return c->fail(HPM_E_INVALID, "hpm_set_prior: bad arguments");
+    cudaSetDevice(c->device);
+    ViewState& v = c->views[view];
+    cudaError_t e = ensure(v.prior, v.prior_cap, (size_t)w * h);
+    if (e == cudaSuccess) e = ensure(v.pmask, v.pmask_cap, (size_t)w * h);
+    if (e != cudaSuccess) return c->cuda_fail(e, "alloc prior");
+    e = cudaMemcpyAsync(v.prior, planes, sizeof(float4) * w * h, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v.pmask, mask, (size_t)w * h, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "upload prior");
+    v.prior_w = w; v.prior_h = h;
+    return HPM_OK;
+}
+
+int hpm_run_patchmatch(hpm_ctx* ctx, int ref, const int32_t* srcs, int n_src, const hpm_params* params,
+                       int texture_level, uint64_t seed) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    return c->run_patchmatch(ref, srcs, n_src, params, texture_level, seed);
+}
+
+int hpm_eval_costs(hpm_ctx* ctx, int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n,
+                   const int32_t* px, const float* planes, float* out) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    return c->eval_costs(ref, srcs, n_src, params, n, px, planes, out);
+}
+
+int hpm_sample_view(hpm_ctx* ctx, int view, int n, const float* xy, float* out) {
+    if (!ctx) return HPM_E_INVALID;
+    return reinterpret_cast<Ctx*>(ctx)->sample_view(view, n, xy, out);
+}
+
+int hpm_debug_run_partial(hpm_ctx* ctx, int ref, const int32_t* srcs, int n_src, const hpm_params* params,
+                          int texture_level, uint64_t seed, int n_half_sweeps, float* planes, float* costs,
+                          uint32_t* selected_views, uint32_t* draws) {
+    if (!ctx) return HPM_E_INVALID;
+    return reinterpret_cast<Ctx*>(ctx)->debug_run_partial(ref, srcs, n_src, params, texture_level, seed,
+                                                          n_half_sweeps, planes, costs, selected_views, draws);
+}
+
+}  // extern "C"

@@ -1,0 +1,81 @@
+// Context object behind the C ABI (hpm_capi.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "hpm_capi.h"
+#include "pm_kernels.cuh"
+
+namespace hpm {
+
+constexpr int kNumMaps = 16;
+
+struct DevMap {
+    float* ptr = nullptr;
+    size_t cap = 0;
+    int w = 0, h = 0, ch = 1;
+};
+
+struct ViewState {
+    int w = 0, h = 0;
+    hpm_camera cam{};
+    float* gray = nullptr;
+    size_t gray_cap = 0;
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+    int arr_w = 0, arr_h = 0, arr_mode = -1;
+    DevMap maps[kNumMaps];
+    uint8_t* canny = nullptr;
+    size_t canny_cap = 0;
+    int canny_w = 0, canny_h = 0;
+    float4* prior = nullptr;
+    size_t prior_cap = 0;
+    uint8_t* pmask = nullptr;
+    size_t pmask_cap = 0;
+    int prior_w = 0, prior_h = 0;
+};
+
+void compute_pose(const hpm_camera& rc, const hpm_camera& sc, ViewPoseH& vp);
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::vector<ViewState> views;
+    int addr_mode = 0;
+    int64_t launches = 0;
+
+    // work buffers of one PatchMatch run (sized for the largest reference view)
+    float4* planes = nullptr; size_t run_cap_planes = 0;
+    float* costs = nullptr; size_t run_cap_costs = 0;
+    float* pre_costs = nullptr; size_t run_cap_pre = 0;
+    uint32_t* sel = nullptr; size_t run_cap_sel = 0;
+    uint32_t* rng = nullptr; size_t run_cap_rng = 0;
+    float* conf = nullptr; size_t run_cap_conf = 0;
+    float4* scaled = nullptr; size_t scaled_cap = 0;
+    uint8_t* scratch = nullptr; size_t scratch_cap = 0;
+
+    ~Ctx();
+    int fail(int code, const char* fmt, ...);
+    int cuda_fail(cudaError_t e, const char* what);
+    cudaError_t ensure_map(int view, int kind, int w, int h);
+    cudaError_t ensure_run(size_t n);
+    int bind_texture(int view);
+    int fill_run_args(int ref, const int32_t* srcs, int n_src, const hpm_params* params, RunArgs& a);
+    int prepare_run(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int texture_level,
+                    uint64_t seed, RunArgs& a);
+    int launch_schedule(const RunArgs& a, int n_half_sweeps);
+    int debug_run_partial(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int texture_level,
+                          uint64_t seed, int n_half_sweeps, float* planes_out, float* costs_out, uint32_t* sel_out,
+                          uint32_t* draws_out);
+    int sample_view(int view, int n, const float* xy, float* out);
+    int run_patchmatch(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int texture_level,
+                       uint64_t seed);
+    int eval_costs(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n, const int32_t* px,
+                   const float* planes, float* out);
+};
+
+}  // namespace hpm

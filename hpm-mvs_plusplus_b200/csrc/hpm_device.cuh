@@ -1,0 +1,329 @@
+// Device-side building blocks of the PatchMatch hot path (sm_100a).
+//
+// The formulas restate HPM-MVS++'s device helpers (HPM.cu:114-564); the
+// structure is new: the reference patch of a pixel (36 texels and their
+// bilateral weights, which do not depend on the hypothesis or the source view)
+// is computed once per pixel per launch and kept in shared memory, so one
+// bilateral NCC costs 36 filtered source fetches plus the moments of the source
+// samples only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "hpm_types.h"
+#include "hpm_philox.h"
+
+namespace hpm {
+
+constexpr int kPatchSamples = 36;   // 11x11 window, stride 2 (HPM.h:231-234)
+constexpr int kPatchRadius = 5;
+constexpr int kPatchStep = 2;
+constexpr int kMarsagliaMaxTries = 4096;
+
+struct PixelRng {
+    uint64_t seed;
+    uint32_t view, x, y, draw;
+    uint32_t block_id;  // draw >> 2 of the cached block, or 0xffffffff
+    uint32_t w[4];
+    __device__ __forceinline__ void init(uint64_t s, uint32_t v, uint32_t px, uint32_t py, uint32_t d) {
+        seed = s; view = v; x = px; y = py; draw = d; block_id = 0xffffffffu;
+    }
+    __device__ __forceinline__ float uniform() {
+        const uint32_t b = draw >> 2;
+        if (b != block_id) {
+            hpm_u32x4 c;
+            c.v[0] = b; c.v[1] = x; c.v[2] = y; c.v[3] = view;
+            const hpm_u32x4 r = hpm_philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+            w[0] = r.v[0]; w[1] = r.v[1]; w[2] = r.v[2]; w[3] = r.v[3];
+            block_id = b;
+        }
+        const uint32_t bits = w[draw & 3u];
+        ++draw;
+        return hpm_bits_to_uniform(bits);
+    }
+};
+
+// ---------------- camera / plane helpers (HPM.cu:114-157, 322-340, 497-537) ----------------
+
+__device__ __forceinline__ float4 rotate_to_world(const hpm_camera& c, float4 p) {
+    float4 r;
+    r.x = c.R[0] * p.x + c.R[3] * p.y + c.R[6] * p.z;
+    r.y = c.R[1] * p.x + c.R[4] * p.y + c.R[7] * p.z;
+    r.z = c.R[2] * p.x + c.R[5] * p.y + c.R[8] * p.z;
+    r.w = p.w;
+    return r;
+}
+
+__device__ __forceinline__ float4 rotate_to_cam(const hpm_camera& c, float4 p) {
+    float4 r;
+    r.x = c.R[0] * p.x + c.R[1] * p.y + c.R[2] * p.z;
+    r.y = c.R[3] * p.x + c.R[4] * p.y + c.R[5] * p.z;
+    r.z = c.R[6] * p.x + c.R[7] * p.y + c.R[8] * p.z;
+    r.w = p.w;
+    return r;
+}
+
+__device__ __forceinline__ float distance_to_origin(const hpm_camera& c, int px, int py, float depth, float4 n) {
+    const float X0 = depth * (px - c.K[2]) / c.K[0];
+    const float X1 = depth * (py - c.K[5]) / c.K[4];
+    return -(n.x * X0 + n.y * X1 + n.z * depth);
+}
+
+__device__ __forceinline__ float depth_from_plane(const hpm_camera& c, float4 pl, int px, int py) {
+    return -pl.w * c.K[0] / ((px - c.K[2]) * pl.x + (c.K[0] / c.K[4]) * (py - c.K[5]) * pl.y + c.K[0] * pl.z);
+}
+
+__device__ __forceinline__ float4 view_direction(const hpm_camera& c, int px, int py, float depth) {
+    const float X0 = depth * (px - c.K[2]) / c.K[0];
+    const float X1 = depth * (py - c.K[5]) / c.K[4];
+    const float X2 = depth;
+    const float norm = sqrtf(X0 * X0 + X1 * X1 + X2 * X2);
+    return make_float4(X0 / norm, X1 / norm, X2 / norm, 0.0f);
+}
+
+__device__ __forceinline__ void normalize3(float4& v) {
+    const float inv = rsqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+    v.x *= inv; v.y *= inv; v.z *= inv;
+}
+
+__device__ __forceinline__ float4 random_normal(const hpm_camera& c, int px, int py, PixelRng& rng, float depth) {
+    float q1 = 1.0f, q2 = 1.0f, s = 2.0f;
+    int tries = 0;
+    while (s >= 1.0f && tries < kMarsagliaMaxTries) {
+        q1 = 2.0f * rng.uniform() - 1.0f;
+        q2 = 2.0f * rng.uniform() - 1.0f;
+        s = q1 * q1 + q2 * q2;
+        ++tries;
+    }
+    if (s >= 1.0f) { q1 = 0.0f; q2 = 0.0f; s = 0.0f; }
+    const float sq = sqrtf(1.0f - s);
+    float4 n = make_float4(2.0f * q1 * sq, 2.0f * q2 * sq, 1.0f - 2.0f * s, 0.0f);
+    const float4 vd = view_direction(c, px, py, depth);
+    if (n.x * vd.x + n.y * vd.y + n.z * vd.z > 0.0f) { n.x = -n.x; n.y = -n.y; n.z = -n.z; }
+    normalize3(n);
+    return n;
+}
+
+__device__ __forceinline__ float4 perturbed_normal(const hpm_camera& c, int px, int py, float4 normal,
+                                                   PixelRng& rng, float perturbation) {
+    const float4 vd = view_direction(c, px, py, 1.0f);
+    const float a1 = (rng.uniform() - 0.5f) * perturbation;
+    const float a2 = (rng.uniform() - 0.5f) * perturbation;
+    const float a3 = (rng.uniform() - 0.5f) * perturbation;
+    float s1, c1, s2, c2, s3, c3;
+    sincosf(a1, &s1, &c1);
+    sincosf(a2, &s2, &c2);
+    sincosf(a3, &s3, &c3);
+    float4 np;
+    np.x = (c2 * c3) * normal.x + (c3 * s1 * s2 - c1 * s3) * normal.y + (s1 * s3 + c1 * c3 * s2) * normal.z;
+    np.y = (c2 * s3) * normal.x + (c1 * c3 + s1 * s2 * s3) * normal.y + (c1 * s2 * s3 - c3 * s1) * normal.z;
+    np.z = (-s2) * normal.x + (c2 * s1) * normal.y + (c1 * c2) * normal.z;
+    np.w = normal.w;
+    if (np.x * vd.x + np.y * vd.y + np.z * vd.z >= 0.0f) np = normal;
+    normalize3(np);
+    return np;
+}
+
+// Per source view, the relative pose terms of ComputeHomography (HPM.cu:251-279)
+// that do not depend on the plane.
+struct ViewPose {
+    float Rr[9];
+    float tr[3];
+};
+
+__device__ __forceinline__ void compute_view_pose(const hpm_camera& rc, const hpm_camera& sc, ViewPose& vp) {
+    float rC[3], sC[3], Cr[3];
+    rC[0] = -(rc.R[0] * rc.t[0] + rc.R[3] * rc.t[1] + rc.R[6] * rc.t[2]);
+    rC[1] = -(rc.R[1] * rc.t[0] + rc.R[4] * rc.t[1] + rc.R[7] * rc.t[2]);
+    rC[2] = -(rc.R[2] * rc.t[0] + rc.R[5] * rc.t[1] + rc.R[8] * rc.t[2]);
+    sC[0] = -(sc.R[0] * sc.t[0] + sc.R[3] * sc.t[1] + sc.R[6] * sc.t[2]);
+    sC[1] = -(sc.R[1] * sc.t[0] + sc.R[4] * sc.t[1] + sc.R[7] * sc.t[2]);
+    sC[2] = -(sc.R[2] * sc.t[0] + sc.R[5] * sc.t[1] + sc.R[8] * sc.t[2]);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            vp.Rr[3 * r + k] = sc.R[3 * r] * rc.R[3 * k] + sc.R[3 * r + 1] * rc.R[3 * k + 1] + sc.R[3 * r + 2] * rc.R[3 * k + 2];
+    Cr[0] = rC[0] - sC[0]; Cr[1] = rC[1] - sC[1]; Cr[2] = rC[2] - sC[2];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+        vp.tr[r] = sc.R[3 * r] * Cr[0] + sc.R[3 * r + 1] * Cr[1] + sc.R[3 * r + 2] * Cr[2];
+}
+
+// Plane-induced homography ref -> src (HPM.cu:281-310) from the hoisted pose.
+__device__ __forceinline__ void plane_homography(const hpm_camera& rc, const hpm_camera& sc, const ViewPose& vp,
+                                                 float4 pl, float H[9]) {
+    float Hm[9], tmp[9];
+    const float n[3] = { pl.x, pl.y, pl.z };
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            Hm[3 * r + k] = vp.Rr[3 * r + k] - vp.tr[r] * n[k] / pl.w;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        tmp[3 * r + 0] = Hm[3 * r + 0] / rc.K[0];
+        tmp[3 * r + 1] = Hm[3 * r + 1] / rc.K[4];
+        tmp[3 * r + 2] = -Hm[3 * r + 0] * rc.K[2] / rc.K[0] - Hm[3 * r + 1] * rc.K[5] / rc.K[4] + Hm[3 * r + 2];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        H[0 + k] = sc.K[0] * tmp[0 + k] + sc.K[2] * tmp[6 + k];
+        H[3 + k] = sc.K[4] * tmp[3 + k] + sc.K[5] * tmp[6 + k];
+        H[6 + k] = sc.K[8] * tmp[6 + k];
+    }
+}
+
+__device__ __forceinline__ float3 point_world(float x, float y, float depth, const hpm_camera& c) {
+    const float X0 = depth * (x - c.K[2]) / c.K[0];
+    const float X1 = depth * (y - c.K[5]) / c.K[4];
+    const float X2 = depth;
+    const float T0 = c.R[0] * X0 + c.R[3] * X1 + c.R[6] * X2;
+    const float T1 = c.R[1] * X0 + c.R[4] * X1 + c.R[7] * X2;
+    const float T2 = c.R[2] * X0 + c.R[5] * X1 + c.R[8] * X2;
+    const float C0 = -(c.R[0] * c.t[0] + c.R[3] * c.t[1] + c.R[6] * c.t[2]);
+    const float C1 = -(c.R[1] * c.t[0] + c.R[4] * c.t[1] + c.R[7] * c.t[2]);
+    const float C2 = -(c.R[2] * c.t[0] + c.R[5] * c.t[1] + c.R[8] * c.t[2]);
+    return make_float3(T0 + C0, T1 + C1, T2 + C2);
+}
+
+__device__ __forceinline__ float2 project_point(float3 X, const hpm_camera& c, float& depth) {
+    const float T0 = c.R[0] * X.x + c.R[1] * X.y + c.R[2] * X.z + c.t[0];
+    const float T1 = c.R[3] * X.x + c.R[4] * X.y + c.R[5] * X.z + c.t[1];
+    const float T2 = c.R[6] * X.x + c.R[7] * X.y + c.R[8] * X.z + c.t[2];
+    depth = c.K[6] * T0 + c.K[7] * T1 + c.K[8] * T2;
+    return make_float2((c.K[0] * T0 + c.K[1] * T1 + c.K[2] * T2) / depth,
+                       (c.K[3] * T0 + c.K[4] * T1 + c.K[5] * T2) / depth);
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ComputeGeomConsistencyCost (HPM.cu:539-564).  The source depth is sampled at
+// texel centres ((int)x + 0.5), i.e. a clamped point fetch.
+__device__ __forceinline__ float geom_cost(const float* __restrict__ sdepth, int sw, int sh, const hpm_camera& rc,
+                                           const hpm_camera& sc, float4 pl, int px, int py) {
+    const float max_cost = 3.0f;
+    const float depth = depth_from_plane(rc, pl, px, py);
+    const float3 fwd = point_world((float)px, (float)py, depth, rc);
+    float sd;
+    const float2 spt = project_point(fwd, sc, sd);
+    const int ix = clampi(__float2int_rz(spt.x), 0, sw - 1);
+    const int iy = clampi(__float2int_rz(spt.y), 0, sh - 1);
+    const float d = __ldg(sdepth + (size_t)iy * sw + ix);
+    if (d == 0.0f) return max_cost;
+    const float3 sX = point_world(spt.x, spt.y, d, sc);
+    float rd;
+    const float2 bwd = project_point(sX, rc, rd);
+    const float dx = px - bwd.x, dy = py - bwd.y;
+    return fminf(max_cost, sqrtf(dx * dx + dy * dy));
+}
+
+// Edge-density texture term (HPM.cu:349-373); the ratio is evaluated in double
+// as in the reference (double literals).
+__device__ __forceinline__ float texture_term(const uint8_t* __restrict__ canny, int W, int H, int px, int py) {
+    int total = 0, edges = 0;
+#pragma unroll
+    for (int i = -5; i < 6; i += 2)
+#pragma unroll
+        for (int j = -5; j < 6; j += 2) {
+            const int x = px + j, y = py + i;
+            if (x >= 0 && x < W && y >= 0 && y < H) {
+                ++total;
+                if (__ldg(canny + (size_t)y * W + x) >= 1) ++edges;
+            }
+        }
+    const float frac = edges * 1.0f / total;
+    return (float)(((double)frac + 0.00005) / ((double)frac + 0.0001));
+}
+
+// Statistics of a pixel's reference patch (view-independent part of the NCC).
+struct RefStats {
+    float mean;      // sum_ref / weight_sum
+    float var;       // reference variance
+    float inv_w;     // 1 / weight_sum
+};
+
+// Loads the reference patch of (px, py) into per-thread shared-memory slots
+// patch[k * stride] = (w_k, w_k * r_k) and returns its statistics.  The weights
+// follow ComputeBilateralWeight (HPM.cu:342-347): unsquared spatial distance and
+// unsquared colour distance over 2*sigma^2.
+__device__ __forceinline__ RefStats load_ref_patch(const float* __restrict__ ref, int W, int H, int px, int py,
+                                                   float sigma_spatial, float sigma_color,
+                                                   float2* patch, int stride) {
+    const float center = __ldg(ref + (size_t)clampi(py, 0, H - 1) * W + clampi(px, 0, W - 1));
+    const float two_ss = 2.0f * sigma_spatial * sigma_spatial;
+    const float two_sc = 2.0f * sigma_color * sigma_color;
+    float s_r = 0.f, s_rr = 0.f, s_w = 0.f;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        float r_r = 0.f, r_rr = 0.f, r_w = 0.f;
+        const int dx = -kPatchRadius + kPatchStep * i;
+        const int x = clampi(px + dx, 0, W - 1);
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const int dy = -kPatchRadius + kPatchStep * j;
+            const float r = __ldg(ref + (size_t)clampi(py + dy, 0, H - 1) * W + x);
+            const float sd = sqrtf((float)(dx * dx + dy * dy));
+            const float w = __expf(-sd / two_ss - fabsf(r - center) / two_sc);
+            const float wr = w * r;
+            patch[(i * 6 + j) * stride] = make_float2(w, wr);
+            r_r += wr;
+            r_rr += wr * r;
+            r_w += w;
+        }
+        s_r += r_r; s_rr += r_rr; s_w += r_w;
+    }
+    RefStats st;
+    st.inv_w = 1.0f / s_w;
+    st.mean = s_r * st.inv_w;
+    st.var = s_rr * st.inv_w - st.mean * st.mean;
+    return st;
+}
+
+// Bilateral NCC of one (pixel, plane, source view) (HPM.cu:375-448) sampling the
+// source through the texture unit (linear filter, clamp).
+__device__ __forceinline__ float ncc_tex(cudaTextureObject_t src, int sw, int sh, const float H[9], int px, int py,
+                                         const RefStats& rs, const float2* patch, int stride) {
+    const float cost_max = 2.0f;
+    {
+        const float cx = H[0] * px + H[1] * py + H[2];
+        const float cy = H[3] * px + H[4] * py + H[5];
+        const float cz = H[6] * px + H[7] * py + H[8];
+        const float ux = cx / cz, uy = cy / cz;
+        if (ux >= sw || ux < 0.0f || uy >= sh || uy < 0.0f) return cost_max;
+    }
+    float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const int x = px - kPatchRadius + kPatchStep * i;
+        float r_s = 0.f, r_ss = 0.f, r_rs = 0.f;
+        float vals[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const int y = py - kPatchRadius + kPatchStep * j;
+            const float qx = H[0] * x + H[1] * y + H[2];
+            const float qy = H[3] * x + H[4] * y + H[5];
+            const float qz = H[6] * x + H[7] * y + H[8];
+            vals[j] = tex2D<float>(src, qx / qz + 0.5f, qy / qz + 0.5f);
+        }
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const float2 wr = patch[(i * 6 + j) * stride];
+            const float s = vals[j];
+            const float ws = wr.x * s;
+            r_s += ws;
+            r_ss += ws * s;
+            r_rs += wr.y * s;
+        }
+        s_s += r_s; s_ss += r_ss; s_rs += r_rs;
+    }
+    s_s *= rs.inv_w; s_ss *= rs.inv_w; s_rs *= rs.inv_w;
+    const float var_s = s_ss - s_s * s_s;
+    const float kMinVar = 1e-5f;
+    if (rs.var < kMinVar || var_s < kMinVar) return cost_max;
+    const float cov = s_rs - rs.mean * s_s;
+    const float vrs = sqrtf(rs.var * var_s);
+    return fmaxf(0.0f, fminf(cost_max, 1.0f - cov / vrs));
+}
+
+}  // namespace hpm

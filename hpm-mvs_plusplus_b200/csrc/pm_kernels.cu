@@ -1,0 +1,836 @@
+// PatchMatch kernels of the plain FP32 path (sm_100a): random initialisation,
+// red/black checkerboard propagation with the non-local sampling pattern, joint
+// view selection and refinement, and the depth/normal export.
+//
+// Algorithm: HPM-MVS++ HPM.cu:567-842 (init, refinement), 843-1873 (standard
+// propagation), 1875-2791 (mandatory consistency), 2793-2842 (schedule,
+// export).  The kernels are laid out differently:
+//   * one thread per pixel of the active colour, block 32 x (BLK/32) over
+//     (x, row pair) so a warp covers a 32 x 2 strip (coherent texture reads);
+//   * the pixel's reference patch (weights and weighted texels) lives in
+//     registers and is built once per launch instead of once per NCC;
+//   * per-pixel cost rows, view weights, final costs and positions live in a
+//     per-thread column of shared memory (stride BLK, conflict-free);
+//   * NCCs whose view weight is zero are not evaluated (their product with the
+//     zero weight is exactly 0 because the NCC is never NaN), and a reference
+//     patch with variance < 1e-5 yields cost 2 for every hypothesis without
+//     sampling (exactly the reference's result).
+// Compiled with --use_fast_math like the reference (CMakeLists.txt:10).
+#include "hpm_device.cuh"
+#include "pm_kernels.cuh"
+
+#include <float.h>
+
+namespace hpm {
+
+static_assert(sizeof(ViewPoseH) == sizeof(ViewPose), "pose layout");
+
+template <int NS, int BLK>
+struct Scratch {
+    float* base;  // smem + threadIdx linear
+    static constexpr int kWords = 9 * NS + 16;
+    __device__ __forceinline__ float& ca(int d, int j) const { return base[(d * NS + j) * BLK]; }
+    __device__ __forceinline__ float& vw(int j) const { return base[(8 * NS + j) * BLK]; }
+    __device__ __forceinline__ float& fc(int d) const { return base[(9 * NS + d) * BLK]; }
+    __device__ __forceinline__ int& pos(int d) const { return reinterpret_cast<int*>(base)[(9 * NS + 8 + d) * BLK]; }
+};
+
+struct Patch {
+    float2 p[kPatchSamples];
+    RefStats rs;
+};
+
+__device__ __forceinline__ void build_patch(const RunArgs& a, int px, int py, Patch& P) {
+    const float* __restrict__ ref = a.ref_img;
+    const int W = a.W, H = a.H;
+    const float center = __ldg(ref + (size_t)clampi(py, 0, H - 1) * W + clampi(px, 0, W - 1));
+    const float two_ss = 2.0f * a.prm.sigma_spatial * a.prm.sigma_spatial;
+    const float two_sc = 2.0f * a.prm.sigma_color * a.prm.sigma_color;
+    float s_r = 0.f, s_rr = 0.f, s_w = 0.f;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        float r_r = 0.f, r_rr = 0.f, r_w = 0.f;
+        const int dx = -kPatchRadius + kPatchStep * i;
+        const int x = clampi(px + dx, 0, W - 1);
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const int dy = -kPatchRadius + kPatchStep * j;
+            const float r = __ldg(ref + (size_t)clampi(py + dy, 0, H - 1) * W + x);
+            const float sd = sqrtf((float)(dx * dx + dy * dy));
+            const float w = __expf(-sd / two_ss - fabsf(r - center) / two_sc);
+            const float wr = w * r;
+            P.p[i * 6 + j] = make_float2(w, wr);
+            r_r += wr;
+            r_rr += wr * r;
+            r_w += w;
+        }
+        s_r += r_r; s_rr += r_rr; s_w += r_w;
+    }
+    P.rs.inv_w = 1.0f / s_w;
+    P.rs.mean = s_r * P.rs.inv_w;
+    P.rs.var = s_rr * P.rs.inv_w - P.rs.mean * P.rs.mean;
+}
+
+// One bilateral NCC (HPM.cu:375-448) with the patch in registers.
+__device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int px, int py, float4 pl, int j) {
+    const float cost_max = 2.0f;
+    if (P.rs.var < 1e-5f) return cost_max;
+    const hpm_camera& rc = a.cams[0];
+    const hpm_camera& sc = a.cams[j + 1];
+    float H[9];
+    plane_homography(rc, sc, reinterpret_cast<const ViewPose&>(a.pose[j + 1]), pl, H);
+    const int sw = sc.width, sh = sc.height;
+    {
+        const float cx = H[0] * px + H[1] * py + H[2];
+        const float cy = H[3] * px + H[4] * py + H[5];
+        const float cz = H[6] * px + H[7] * py + H[8];
+        const float ux = cx / cz, uy = cy / cz;
+        if (ux >= sw || ux < 0.0f || uy >= sh || uy < 0.0f) return cost_max;
+    }
+    const cudaTextureObject_t tex = a.tex[j + 1];
+    float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        const int x = px - kPatchRadius + kPatchStep * i;
+        float v[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const int y = py - kPatchRadius + kPatchStep * k;
+            const float qx = H[0] * x + H[1] * y + H[2];
+            const float qy = H[3] * x + H[4] * y + H[5];
+            const float qz = H[6] * x + H[7] * y + H[8];
+            v[k] = tex2D<float>(tex, qx / qz + 0.5f, qy / qz + 0.5f);
+        }
+        float r_s = 0.f, r_ss = 0.f, r_rs = 0.f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float2 w = P.p[i * 6 + k];
+            const float ws = w.x * v[k];
+            r_s += ws;
+            r_ss += ws * v[k];
+            r_rs += w.y * v[k];
+        }
+        s_s += r_s; s_ss += r_ss; s_rs += r_rs;
+    }
+    s_s *= P.rs.inv_w; s_ss *= P.rs.inv_w; s_rs *= P.rs.inv_w;
+    const float var_s = s_ss - s_s * s_s;
+    if (var_s < 1e-5f) return cost_max;
+    const float cov = s_rs - P.rs.mean * s_s;
+    const float vrs = sqrtf(P.rs.var * var_s);
+    return fmaxf(0.0f, fminf(cost_max, 1.0f - cov / vrs));
+}
+
+// ---------------------------------------------------------------- init
+
+template <int NS, int BLK>
+__device__ float initial_cost(const RunArgs& a, const Patch& P, int px, int py, float4 pl, uint32_t* sel_out,
+                              const Scratch<NS, BLK>& s) {
+    const float cost_max = 2.0f;
+    const int S = a.S;
+    int valid = 0;
+    for (int j = 0; j < S; ++j) {
+        const float c = ncc_view(a, P, px, py, pl, j);
+        s.ca(0, j) = c;
+        s.ca(1, j) = c;
+        if (c < cost_max) ++valid;
+    }
+    // insertion sort of row 1 (HPM.cu:15-24)
+    for (int i = 1; i < S; ++i) {
+        const float t = s.ca(1, i);
+        int k = i;
+        for (; k >= 1 && t < s.ca(1, k - 1); --k) s.ca(1, k) = s.ca(1, k - 1);
+        s.ca(1, k) = t;
+    }
+    uint32_t sel = 0;
+    const int top_k = min(valid, a.prm.top_k);
+    float result = cost_max;
+    if (top_k > 0) {
+        float cost = 0.0f;
+        for (int i = 0; i < top_k; ++i) cost += s.ca(1, i);
+        const float thr = s.ca(1, top_k - 1);
+        for (int i = 0; i < S; ++i)
+            if (s.ca(0, i) <= thr) sel |= (1u << i);
+        result = cost / top_k;
+    }
+    *sel_out = sel;
+    return result;
+}
+
+__device__ __forceinline__ float spatial_gauss(float x1, float y1, float x2, float y2, float sigma) {
+    const float dx = x1 - x2, dy = y1 - y2;
+    const float dis = dx * dx + dy * dy - 0.0f;
+    return (float)exp(-1.0 * dis / (2 * sigma * sigma));
+}
+
+__device__ __forceinline__ float range_gauss(float x, float sigma) {
+    return (float)exp(-1.0 * (x * x) / (2 * sigma * sigma));
+}
+
+template <int NS, int BLK>
+__global__ void __launch_bounds__(BLK) k_random_init(const __grid_constant__ RunArgs a) {
+    extern __shared__ float smem[];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    Scratch<NS, BLK> s{ smem + tid };
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
+    const int W = a.W, H = a.H;
+    if (px >= W || py >= H) return;
+    const int center = py * W + px;
+    const hpm_camera& c0 = a.cams[0];
+    const uint32_t mode = a.prm.mode;
+    const bool geom = mode & HPM_MODE_GEOM, prior = mode & HPM_MODE_PRIOR, hier = mode & HPM_MODE_HIERARCHY;
+    const bool ups = mode & HPM_MODE_UPSAMPLE, mand = mode & HPM_MODE_MAND;
+    PixelRng rng;
+    rng.init(a.seed, a.view_id, px, py, 0);
+
+    if (!prior && !mand) a.texture[center] = texture_term(a.canny, W, H, px, py);
+
+    Patch P;
+    build_patch(a, px, py, P);
+    uint32_t sel = 0;
+    if (!geom && !hier && !prior) {
+        const float depth = rng.uniform() * (a.prm.depth_max - a.prm.depth_min) + a.prm.depth_min;
+        float4 pl = random_normal(c0, px, py, rng, depth);
+        pl.w = distance_to_origin(c0, px, py, depth, pl);
+        a.planes[center] = pl;
+        a.costs[center] = initial_cost(a, P, px, py, pl, &sel, s);
+        a.sel[center] = sel;
+    } else if (prior) {
+        if (a.pmask[center] > 0) {
+            if (a.conf[center] > 0.3) {
+                float4 pl = a.planes[center];
+                pl.w = distance_to_origin(c0, px, py, pl.w, pl);
+                a.planes[center] = pl;
+                a.costs[center] = 0.1f;
+            } else if (a.costs[center] > 0.1f) {
+                const float perturbation = 0.02f;
+                const float4 pp = a.prior[center];
+                float dp = pp.w;  // the prior's offset is used as a depth (HPM.cu:603-604)
+                const float dmin_p = (1 - 3 * perturbation) * dp;
+                const float dmax_p = (1 + 3 * perturbation) * dp;
+                dp = rng.uniform() * (dmax_p - dmin_p) + dmin_p;
+                float4 pl = perturbed_normal(c0, px, py, pp, rng, (float)(3 * perturbation * 3.14159265358979323846));
+                pl.w = dp;
+                a.planes[center] = pl;
+                a.costs[center] = initial_cost(a, P, px, py, pl, &sel, s);
+                a.sel[center] = sel;
+            } else {
+                float4 pl = a.planes[center];
+                pl.w = distance_to_origin(c0, px, py, pl.w, pl);
+                a.planes[center] = pl;
+                a.costs[center] = initial_cost(a, P, px, py, pl, &sel, s);
+                a.sel[center] = sel;
+            }
+        } else {
+            float4 pl = a.planes[center];
+            pl.w = distance_to_origin(c0, px, py, pl.w, pl);
+            a.planes[center] = pl;
+            if (a.conf[center] > 0.3) a.costs[center] = 0.1f;
+        }
+    } else if (ups) {
+        const int scols = a.prm.scaled_cols, srows = a.prm.scaled_rows;
+        const float sc_f = (float)scols, sr_f = (float)srows;
+        const float scale = (float)(1.0 * sc_f / W);
+        const float sigmad = 0.50f, sigmar = 25.5f;
+        const int image_scale = (int)fmaxf(W / sc_f, H / sr_f);
+        const int nn = (image_scale * image_scale + 1) / 2;
+        const float o_y = py * scale, o_x = px * scale;
+        const float ref_pix = __ldg(a.ref_img + center);
+        float nf = 0.0f;
+        float n0 = 0.0f, n1 = 0.0f, n2 = 0.0f;
+        for (int j = -nn; j <= nn; ++j) {
+            int r_y = __float2int_rz(o_y + j);
+            r_y = (r_y > 0 ? (r_y < sr_f ? r_y : srows - 1) : 0);
+            const int r_ys = clampi(py + j, 0, H - 1);
+            for (int i = -nn; i <= nn; ++i) {
+                int r_x = __float2int_rz(o_x + i);
+                r_x = (r_x > 0 ? (r_x < sc_f ? r_x : scols - 1) : 0);
+                const int s_center = (int)(r_y * sc_f + r_x);
+                const float4 sn = a.scaled[s_center];
+                const float nb = __ldg(a.ref_img + (size_t)r_ys * W + clampi(px + i, 0, W - 1));
+                const float tg = spatial_gauss(o_x, o_y, (float)r_x, (float)r_y, sigmad) *
+                                 range_gauss(fabsf(ref_pix - nb), sigmar);
+                nf += tg;
+                n0 = n0 + sn.x * tg; n1 = n1 + sn.y * tg; n2 = n2 + sn.z * tg;
+            }
+        }
+        float4 nt = make_float4(n0 / nf, n1 / nf, n2 / nf, 0.0f);
+        normalize3(nt);
+        const float4 cur = a.planes[center];
+        // pre-cost plane: zero normal, upsampled depth as offset (HPM.cu:689, HPM.cpp:894-901)
+        const float pre = initial_cost(a, P, px, py, make_float4(0.f, 0.f, 0.f, cur.w), &sel, s);
+        a.pre_costs[center] = pre;
+        float4 pl = rotate_to_cam(c0, nt);
+        pl.w = distance_to_origin(c0, px, py, cur.w, pl);
+        a.planes[center] = pl;
+        a.costs[center] = initial_cost(a, P, px, py, pl, &sel, s);
+        a.sel[center] = sel;
+    } else {
+        if (mand && !(a.conf[center] >= 0.3)) {
+            if (texture_term(a.canny, W, H, px, py) > 0.5) a.conf[center] = 0.1f;
+        }
+        float4 pl = hier ? a.scaled[center] : a.planes[center];
+        pl = rotate_to_cam(c0, pl);
+        pl.w = distance_to_origin(c0, px, py, pl.w, pl);
+        a.planes[center] = pl;
+        a.costs[center] = initial_cost(a, P, px, py, pl, &sel, s);
+        a.sel[center] = sel;
+    }
+    a.rng[center] = rng.draw;
+}
+
+// ---------------------------------------------------------------- propagation
+
+template <int NS, int BLK>
+__device__ __forceinline__ void cost_row(const RunArgs& a, const Patch& P, int px, int py, float4 pl, int d,
+                                         const Scratch<NS, BLK>& s) {
+    for (int j = 0; j < a.S; ++j) s.ca(d, j) = ncc_view(a, P, px, py, pl, j);
+}
+
+__device__ __forceinline__ void v_path_scan(const float* __restrict__ costs, int W, int H, int x, int y, int ax,
+                                            int ay, int bx, int by, float& bc, int& best) {
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        if (i % 2 == 0) { x += ax; y += ay; } else { x += bx; y += by; }
+        if (x >= 0 && x < W && y < H && y >= 0) {
+            const int q = y * W + x;
+            const float c = costs[q];
+            if (c < bc) { bc = c; best = q; }
+        } else break;
+    }
+}
+
+// First candidate 5 px away along (dx, dy), then up to 4 more every 2 px while
+// inside the image (HPM.cu:1385-1475).  right_far keeps the maximum (HPM.cu:1464).
+__device__ __forceinline__ bool far_search(const float* __restrict__ costs, int W, int H, int px, int py, int dx,
+                                           int dy, bool keep_max, int& pos) {
+    const int x = px + 5 * dx, y = py + 5 * dy;
+    if (x < 0 || x >= W || y < 0 || y >= H) return false;
+    int best = y * W + x;
+    float bc = costs[best];
+#pragma unroll
+    for (int i = 1; i < 5; ++i) {
+        const int xi = px + (5 + 2 * i) * dx, yi = py + (5 + 2 * i) * dy;
+        if (xi < 0 || xi >= W || yi < 0 || yi >= H) break;
+        const int q = yi * W + xi;
+        const float c = costs[q];
+        if (keep_max ? (bc < c) : (c < bc)) { bc = c; best = q; }
+    }
+    pos = best;
+    return true;
+}
+
+struct CommonOut {
+    uint32_t flags;        // bit d: direction d valid
+    uint32_t temp_selected;
+    int num_selected;
+    float weight_norm;
+};
+
+// Direction search, extension, joint view selection and final costs
+// (HPM.cu:1367-1771); shared by both propagation variants.
+template <int NS, int BLK>
+__device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, int py, int iter, PixelRng& rng,
+                                      const Scratch<NS, BLK>& s) {
+    const int W = a.W, H = a.H, S = a.S;
+    const int center = py * W + px;
+    const float* __restrict__ costs = a.costs;
+    const bool geom = a.prm.mode & HPM_MODE_GEOM;
+    CommonOut o;
+    o.flags = 0;
+
+    // `float cost_array[8][32] = { 2.0f }` (HPM.cu:1378): only [0][0] is 2, the rest 0.
+    for (int d = 0; d < 8; ++d)
+        for (int j = 0; j < S; ++j) s.ca(d, j) = 0.0f;
+    s.ca(0, 0) = 2.0f;
+
+    int pos[8];
+    pos[0] = center - 5 - 6 * W; pos[1] = center - 5 * W; pos[2] = center + 6 - 5 * W; pos[3] = center + 5 * W;
+    pos[4] = center + 5 + 6 * W; pos[5] = center - 5; pos[6] = center - 6 + 5 * W; pos[7] = center + 5;
+    if (far_search(costs, W, H, px, py, 0, -1, false, pos[1])) o.flags |= 1u << 1;
+    if (far_search(costs, W, H, px, py, 0, 1, false, pos[3])) o.flags |= 1u << 3;
+    if (far_search(costs, W, H, px, py, -1, 0, false, pos[5])) o.flags |= 1u << 5;
+    if (far_search(costs, W, H, px, py, 1, 0, true, pos[7])) o.flags |= 1u << 7;
+    if (px > 4 && py > 5) {
+        o.flags |= 1u << 0;
+        float bc = costs[pos[0]]; int best = pos[0];
+        v_path_scan(costs, W, H, px - 5, py - 6, -2, 0, 0, -2, bc, best);
+        pos[0] = best;
+    }
+    if (px < W - 6 && py > 4) {
+        o.flags |= 1u << 2;
+        float bc = costs[pos[2]]; int best = pos[2];
+        v_path_scan(costs, W, H, px + 6, py - 5, 0, -2, 2, 0, bc, best);
+        pos[2] = best;
+    }
+    if (px < W - 5 && py < H - 6) {
+        o.flags |= 1u << 4;
+        float bc = costs[pos[4]]; int best = pos[4];
+        v_path_scan(costs, W, H, px + 5, py + 6, 2, 0, 0, 2, bc, best);
+        pos[4] = best;
+    }
+    if (px > 5 && py < H - 5) {
+        o.flags |= 1u << 6;
+        float bc = costs[pos[6]]; int best = pos[6];
+        v_path_scan(costs, W, H, px - 6, py + 5, 0, 2, -2, 0, bc, best);
+        pos[6] = best;
+    }
+#pragma unroll
+    for (int d = 0; d < 8; ++d) s.pos(d) = pos[d];
+
+    for (int d = 0; d < 8; ++d) {
+        if (o.flags & (1u << d)) cost_row(a, P, px, py, a.planes[s.pos(d)], d, s);
+    }
+
+    // Extended propagation: only orientation 0 (left_up) is active because
+    // `bool symbol_eight_orientations[10] = { true }` (HPM.cu:1612, 1063-1126).
+    if (o.flags & 1u) {
+        for (int it = 0; it < 3; ++it) {
+            const float good_thr = (float)(0.8 * exp(-iter * iter * (3 - it) / 90.0));
+            int good = 0, bad = 0;
+            for (int j = 0; j < S; ++j) {
+                const float c = s.ca(0, j);
+                if (c < good_thr) ++good;
+                if (c > 1.2f) ++bad;
+            }
+            if (good >= 1 && bad <= 2) break;
+            if (px > 4 + 8 * it && py > 5 + 8 * it) {
+                const int sx = px - 5 - 8 * it, sy = py - 6 - 8 * it;
+                int best = sy * W + sx;
+                float bc = costs[best];
+                v_path_scan(costs, W, H, sx, sy, -2, 0, 0, -2, bc, best);
+                const int prev = s.pos(0);
+                if (bc > costs[prev]) {
+                    best = prev;
+                } else if (best != prev) {
+                    cost_row(a, P, px, py, a.planes[best], 0, s);
+                }
+                // best == prev recomputes the same row in the reference: identical values
+                s.pos(0) = best;
+            }
+        }
+    }
+
+    // Joint view selection (HPM.cu:1686-1751)
+    float priors[NS];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) priors[j] = 0.0f;
+    const int nbr[4] = { center - W * 5, center + W * 5, center - 5, center + 5 };
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        if (o.flags & (1u << (2 * i + 1))) {
+            const uint32_t m = a.sel[nbr[i]];
+#pragma unroll
+            for (int j = 0; j < NS; ++j)
+                if (j < S) priors[j] += ((m >> j) & 1u) ? 0.9f : 0.1f;
+        }
+    }
+    const float cost_thr = (float)(0.8 * __expf((float)(iter * iter) / (-90.0f)));
+    float probs[NS];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        probs[j] = 0.0f;
+        if (j < S) {
+            float count = 0.0f, tmpw = 0.0f;
+            int count_false = 0;
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                const float c = s.ca(d, j);
+                if (c < cost_thr) { tmpw += __expf(c * c / (-0.18f)); count += 1.0f; }
+                if (c > 1.2f) ++count_false;
+            }
+            if (count > 2 && count_false < 3) probs[j] = tmpw / count;
+            else if (count_false < 3) probs[j] = __expf(cost_thr * cost_thr / (-0.32f));
+            probs[j] = probs[j] * priors[j];
+        }
+    }
+    {
+        float sum = 0.0f;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) if (j < S) sum += probs[j];
+        const float inv = 1.0f / sum;
+        float cum = 0.0f;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) if (j < S) { cum += probs[j] * inv; probs[j] = cum; }
+    }
+    float vw[NS];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) vw[j] = 0.0f;
+    for (int smp = 0; smp < 15; ++smp) {
+        const float rp = rng.uniform() - FLT_EPSILON;
+        bool done = false;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            if (!done && j < S && probs[j] > rp) { vw[j] += 1.0f; done = true; }
+        }
+    }
+    o.temp_selected = 0; o.num_selected = 0; o.weight_norm = 0.0f;
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        s.vw(j) = vw[j];
+        if (j < S && vw[j] > 0) {
+            o.temp_selected |= 1u << j;
+            o.weight_norm += vw[j];
+            o.num_selected++;
+        }
+    }
+    for (int d = 0; d < 8; ++d) {
+        float fc = 0.0f;
+        const bool valid = o.flags & (1u << d);
+        float4 pl = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (geom && valid) pl = a.planes[s.pos(d)];
+        for (int j = 0; j < S; ++j) {
+            const float w = s.vw(j);
+            if (w > 0) {
+                if (geom) {
+                    if (valid)
+                        fc += w * (s.ca(d, j) + 0.2f * geom_cost(a.depth_src[j + 1], a.dsw[j + 1], a.dsh[j + 1],
+                                                                   a.cams[0], a.cams[j + 1], pl, px, py));
+                    else
+                        fc += w * (s.ca(d, j) + 0.1f * 3.0f);
+                } else {
+                    fc += w * s.ca(d, j);
+                }
+            }
+        }
+        s.fc(d) = fc / o.weight_norm;
+    }
+    return o;
+}
+
+// Weighted cost of plane pl over the selected views (HPM.cu:1775-1786).
+template <int NS, int BLK>
+__device__ __forceinline__ float selected_cost(const RunArgs& a, const Patch& P, int px, int py, float4 pl,
+                                               uint32_t selmask, float weight_norm, const Scratch<NS, BLK>& s) {
+    const bool geom = a.prm.mode & HPM_MODE_GEOM;
+    float c = 0.0f;
+    for (int j = 0; j < a.S; ++j) {
+        if (!((selmask >> j) & 1u)) continue;
+        const float w = s.vw(j);
+        const float n = ncc_view(a, P, px, py, pl, j);
+        if (geom) c += w * (n + 0.2f * geom_cost(a.depth_src[j + 1], a.dsw[j + 1], a.dsh[j + 1], a.cams[0],
+                                                  a.cams[j + 1], pl, px, py));
+        else c += w * n;
+    }
+    return c / weight_norm;
+}
+
+__device__ __forceinline__ int find_min_index8(const float* v) {  // ties -> last (HPM.cu:41-52)
+    float m = v[0]; int idx = 0;
+#pragma unroll
+    for (int i = 1; i < 8; ++i) if (v[i] <= m) { m = v[i]; idx = i; }
+    return idx;
+}
+
+__device__ __forceinline__ int find_max_index8(const float* v) {  // ties -> last (HPM.cu:54-65)
+    float m = v[0]; int idx = 0;
+#pragma unroll
+    for (int i = 1; i < 8; ++i) if (v[i] >= m) { m = v[i]; idx = i; }
+    return idx;
+}
+
+__device__ __forceinline__ float prior_score(float final_cost, float depth_now, float depth_prior, float4 pp,
+                                             float4 pl, float texture, float two_dss, float two_ass) {
+    const float gamma = 0.5f, beta = 0.18f;
+    const float dd = depth_now - depth_prior;
+    const float nd = fabsf(pp.x - pl.x) + fabsf(pp.y - pl.y) + fabsf(pp.z - pl.z);
+    const float prior = (float)(gamma * (1.2 - 0.2 * texture) + (double)(__expf(-dd * dd / two_dss) * __expf(-nd * nd / two_ass)));
+    return (float)(exp(-final_cost * final_cost / beta * (1 + 0.2 * texture)) * (double)prior);
+}
+
+// PlaneHypothesisRefinement (HPM.cu:765-841).  The five candidates are built
+// from the state at entry, evaluated in order and accepted greedily.
+template <int NS, int BLK>
+__device__ void refinement(const RunArgs& a, const Patch& P, int px, int py, float4& plane, float& depth,
+                           float& cost, PixelRng& rng, uint32_t selmask, float weight_norm, float* restricted_cost,
+                           float texture, const Scratch<NS, BLK>& s) {
+    const hpm_camera& c0 = a.cams[0];
+    const int center = py * a.W + px;
+    const bool prior = a.prm.mode & HPM_MODE_PRIOR;
+    const float perturbation = 0.02f;
+    const float dmin = a.prm.depth_min, dmax = a.prm.depth_max;
+    const float depth_sigma = (dmax - dmin) / 64.0f;
+    const float two_dss = 2 * depth_sigma * depth_sigma;
+    const float angle_sigma = (float)(3.14159265358979323846 * (5.0f / 180.0f));
+    const float two_ass = 2 * angle_sigma * angle_sigma;
+    float depth_prior = 0.0f, depth_rand;
+    float4 plane_rand;
+    const bool use_prior = prior && a.pmask[center] > 0;
+    float4 pp = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (use_prior) {
+        pp = a.prior[center];
+        depth_prior = depth_from_plane(c0, pp, px, py);
+        depth_rand = rng.uniform() * 6 * depth_sigma + (depth_prior - 3 * depth_sigma);
+        plane_rand = perturbed_normal(c0, px, py, pp, rng, angle_sigma);
+    } else {
+        depth_rand = rng.uniform() * (dmax - dmin) + dmin;
+        plane_rand = random_normal(c0, px, py, rng, depth);
+    }
+    const float dmin_p = (1 - perturbation) * depth;
+    const float dmax_p = (1 + perturbation) * depth;
+    const float depth_perturbed = rng.uniform() * (dmax_p - dmin_p) + dmin_p;
+    const float4 plane_perturbed =
+        perturbed_normal(c0, px, py, plane, rng, (float)(perturbation * 3.14159265358979323846));
+    const float depths5[5] = { depth_rand, depth, depth_rand, depth, depth_perturbed };
+    const float4 normals5[5] = { plane, plane_rand, plane_rand, plane_perturbed, plane };
+#pragma unroll 1
+    for (int i = 0; i < 5; ++i) {
+        float4 t = normals5[i];
+        t.w = distance_to_origin(c0, px, py, depths5[i], t);
+        const float tc = selected_cost(a, P, px, py, t, selmask, weight_norm, s);
+        const float db = depth_from_plane(c0, t, px, py);
+        if (use_prior) {
+            const float rt = prior_score(tc, depths5[i], depth_prior, pp, t, texture, two_dss, two_ass);
+            if (db >= dmin && db <= dmax && rt > *restricted_cost) {
+                depth = db; plane = t; cost = tc; *restricted_cost = rt;
+            }
+        } else if (db >= dmin && db <= dmax && tc < cost) {
+            depth = db; plane = t; cost = tc;
+        }
+    }
+}
+
+template <int NS, int BLK, bool MAND>
+__global__ void __launch_bounds__(BLK) k_half_sweep(const __grid_constant__ RunArgs a, int color, int iter) {
+    extern __shared__ float smem[];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const Scratch<NS, BLK> s{ smem + tid };
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int pair = blockIdx.y * blockDim.y + threadIdx.y;
+    const int py = 2 * pair + ((px & 1) ^ color);
+    const int W = a.W, H = a.H;
+    if (px >= W || py >= H || pair >= a.cover_pairs) return;
+    const int center = py * W + px;
+    const hpm_camera& c0 = a.cams[0];
+    const uint32_t mode = a.prm.mode;
+    const bool prior = mode & HPM_MODE_PRIOR, hier = mode & HPM_MODE_HIERARCHY;
+    const float dmin = a.prm.depth_min, dmax = a.prm.depth_max;
+
+    if (!MAND && prior) {
+        if (a.conf[center] > 0.3) return;
+        if (a.pmask[center] == 0) return;
+    }
+    PixelRng rng;
+    rng.init(a.seed, a.view_id, px, py, a.rng[center]);
+    Patch P;
+    build_patch(a, px, py, P);
+    const bool reliable = MAND ? (a.conf[center] >= 0.3) : true;
+    const CommonOut o = propagate_common<NS, BLK>(a, P, px, py, iter, rng, s);
+    float fcl[8];
+#pragma unroll
+    for (int d = 0; d < 8; ++d) fcl[d] = s.fc(d);
+
+    if (!MAND || reliable) {
+        const int min_idx = find_min_index8(fcl);
+        const bool min_valid = o.flags & (1u << min_idx);
+        float4 cur = a.planes[center];
+        float cost_now = selected_cost(a, P, px, py, cur, o.temp_selected, o.weight_norm, s);
+        a.costs[center] = cost_now;
+        const float cost_chk = cost_now;  // costs[center] as read by the NaN test
+        float depth_now = depth_from_plane(c0, cur, px, py);
+        float restricted_cost = 0.0f;
+        float texture = 0.0f;
+        float cost_store = cost_now;  // costs[center] before the final write
+        if (!MAND && prior) {
+            const float depth_sigma = (dmax - dmin) / 64.0f;
+            const float two_dss = 2 * depth_sigma * depth_sigma;
+            const float angle_sigma = (float)(3.14159265358979323846 * (5.0f / 180.0f));
+            const float two_ass = 2 * angle_sigma * angle_sigma;
+            const float4 pp = a.prior[center];
+            const float depth_prior = depth_from_plane(c0, pp, px, py);
+            texture = texture_term(a.canny, W, H, px, py);
+            if (a.pmask[center] > 0) {
+                float rfc[8];
+#pragma unroll
+                for (int d = 0; d < 8; ++d) {
+                    rfc[d] = 0.0f;
+                    if (o.flags & (1u << d)) {
+                        const float4 pl = a.planes[s.pos(d)];
+                        const float dn = depth_from_plane(c0, pl, px, py);
+                        rfc[d] = prior_score(fcl[d], dn, depth_prior, pp, pl, texture, two_dss, two_ass);
+                    }
+                }
+                const int max_idx = find_max_index8(rfc);
+                const float rnow = prior_score(cost_now, depth_now, depth_prior, pp, cur, texture, two_dss, two_ass);
+                if (o.flags & (1u << max_idx)) {
+                    const float4 pl = a.planes[s.pos(max_idx)];
+                    const float db = depth_from_plane(c0, pl, px, py);
+                    if (db >= dmin && db <= dmax && rfc[max_idx] > rnow) {
+                        depth_now = db;
+                        cur = pl;
+                        a.planes[center] = pl;
+                        cost_store = fcl[max_idx];
+                        a.costs[center] = cost_store;
+                        restricted_cost = rfc[max_idx];
+                        a.sel[center] = o.temp_selected;
+                    }
+                }
+            } else if (min_valid) {
+                const float4 pl = a.planes[s.pos(min_idx)];
+                const float db = depth_from_plane(c0, pl, px, py);
+                if (db >= dmin && db <= dmax && fcl[min_idx] < cost_now) {
+                    depth_now = db;
+                    cur = pl;
+                    a.planes[center] = pl;
+                    cost_store = fcl[min_idx];
+                    a.costs[center] = cost_store;
+                }
+            }
+        }
+        // plane_hypotheses_now is uninitialised in the reference (HPM.cu:1844, 2299); it
+        // starts as the pixel's current plane here.
+        float4 plane_now = cur;
+        if ((MAND || !prior) && min_valid) {
+            const float4 pl = a.planes[s.pos(min_idx)];
+            const float db = depth_from_plane(c0, pl, px, py);
+            if (db >= dmin && db <= dmax && fcl[min_idx] < cost_now) {
+                depth_now = db; plane_now = pl; cost_now = fcl[min_idx];
+                a.sel[center] = o.temp_selected;
+            }
+            if (cost_chk != cost_chk) {
+                if (!MAND) depth_now = db;
+                plane_now = pl; cost_now = fcl[min_idx];
+                a.sel[center] = o.temp_selected;
+            }
+        }
+        refinement(a, P, px, py, plane_now, depth_now, cost_now, rng, o.temp_selected, o.weight_norm,
+                   &restricted_cost, texture, s);
+        if (!MAND && hier) {
+            if (cost_now < a.pre_costs[center] - 0.1f) {
+                a.costs[center] = cost_now;
+                a.planes[center] = plane_now;
+            }
+        } else {
+            a.costs[center] = cost_now;
+            a.planes[center] = plane_now;
+        }
+        (void)cost_store;
+    } else {
+        // mandatory consistency, unreliable pixel (HPM.cu:2684-2789)
+        const float beta = 0.18f;
+        float rfc[8];
+        const float mmc = o.num_selected * 0.5f;
+#pragma unroll
+        for (int d = 0; d < 8; ++d) {
+            rfc[d] = 0.0f;
+            if (o.flags & (1u << d)) {
+                const float cp = a.conf[s.pos(d)];
+                const float gce = __expf(-fcl[d] * fcl[d] / beta);
+                const float dm = fmaxf(0.0f, mmc - cp);
+                const float mce = (float)(0.5f + exp(-dm * dm / (mmc * mmc * 1.0)));
+                rfc[d] = (cp > 0) ? fmaxf(3.0f, mce) * gce : mce * gce;
+                if (cp > 0) fcl[d] = (float)(fcl[d] * fmin((double)__expf(-cp * 2), 0.35));
+            }
+        }
+        const int max_idx = find_max_index8(rfc);
+        const float4 cur = a.planes[center];
+        float cost_now = selected_cost(a, P, px, py, cur, o.temp_selected, o.weight_norm, s);
+        const float cost_chk = cost_now;
+        const float cc = a.conf[center];
+        const float gce = __expf(-cost_now * cost_now / beta);
+        const float dm = fmaxf(0.0f, mmc - cc);
+        const float mce = (float)(0.5f + exp(-dm * dm / (mmc * mmc * 1.0)));
+        const float rnow = (cc > 0) ? fmaxf(3.0f, mce) * gce : mce * gce;
+        if (cc < 0.3) cost_now = (float)(cost_now * exp(0.2 + cc * 2));
+        else cost_now = cost_now * __expf(-cc * 2);
+        float4 plane_now = cur;  // uninitialised in the reference (HPM.cu:2761)
+        if (o.flags & (1u << max_idx)) {
+            const int pm = s.pos(max_idx);
+            const float4 pl = a.planes[pm];
+            const float db = depth_from_plane(c0, pl, px, py);
+            if (db >= dmin && db <= dmax && rfc[max_idx] > rnow) {
+                plane_now = pl; cost_now = fcl[max_idx];
+                a.sel[center] = o.temp_selected;
+                a.conf[center] = (float)(0.5 * a.conf[pm]);
+            }
+            if (cost_chk != cost_chk) {
+                plane_now = pl; cost_now = fcl[max_idx];
+                a.sel[center] = o.temp_selected;
+                a.conf[center] = (float)(0.5 * a.conf[pm]);
+            }
+        }
+        a.costs[center] = cost_now;
+        a.planes[center] = plane_now;
+    }
+    a.rng[center] = rng.draw;
+}
+
+__global__ void k_export(const __grid_constant__ RunArgs a) {
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int py = blockIdx.y * blockDim.y + threadIdx.y;
+    if (px >= a.W || py >= a.H) return;
+    const int center = py * a.W + px;
+    float4 pl = a.planes[center];
+    pl.w = depth_from_plane(a.cams[0], pl, px, py);
+    a.planes[center] = rotate_to_world(a.cams[0], pl);
+}
+
+__global__ void k_eval_costs(const __grid_constant__ RunArgs a, int n, const int32_t* __restrict__ px,
+                             const float4* __restrict__ planes, float* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int x = px[2 * k], y = px[2 * k + 1];
+    Patch P;
+    build_patch(a, x, y, P);
+    const float4 pl = planes[k];
+    for (int j = 0; j < a.S; ++j) out[(size_t)k * a.S + j] = ncc_view(a, P, x, y, pl, j);
+}
+
+// ---------------------------------------------------------------- launchers
+
+template <int NS>
+static constexpr int block_threads() { return NS <= 10 ? 128 : (NS <= 16 ? 64 : 32); }
+
+template <int NS>
+static cudaError_t init_impl(const RunArgs& a, cudaStream_t st) {
+    constexpr int BLK = 128;
+    const size_t shm = sizeof(float) * Scratch<NS, BLK>::kWords * BLK;
+    auto k = k_random_init<NS, BLK>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    if (e != cudaSuccess) return e;
+    dim3 block(16, 8), grid((a.W + 15) / 16, (a.H + 7) / 8);
+    k<<<grid, block, shm, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int NS, bool MAND>
+static cudaError_t sweep_impl(const RunArgs& a, int color, int iter, cudaStream_t st) {
+    constexpr int BLK = block_threads<NS>();
+    const size_t shm = sizeof(float) * Scratch<NS, BLK>::kWords * BLK;
+    auto k = k_half_sweep<NS, BLK, MAND>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    if (e != cudaSuccess) return e;
+    dim3 block(32, BLK / 32), grid((a.W + 31) / 32, (a.cover_pairs + BLK / 32 - 1) / (BLK / 32));
+    k<<<grid, block, shm, st>>>(a, color, iter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_random_init(const RunArgs& a, cudaStream_t st) {
+    if (a.S <= 4) return init_impl<4>(a, st);
+    if (a.S <= 10) return init_impl<10>(a, st);
+    if (a.S <= 16) return init_impl<16>(a, st);
+    return init_impl<31>(a, st);
+}
+
+cudaError_t launch_half_sweep(const RunArgs& a, int color, int iter, cudaStream_t st) {
+    const bool mand = a.prm.mode & HPM_MODE_MAND;
+    if (a.S <= 4) return mand ? sweep_impl<4, true>(a, color, iter, st) : sweep_impl<4, false>(a, color, iter, st);
+    if (a.S <= 10) return mand ? sweep_impl<10, true>(a, color, iter, st) : sweep_impl<10, false>(a, color, iter, st);
+    if (a.S <= 16) return mand ? sweep_impl<16, true>(a, color, iter, st) : sweep_impl<16, false>(a, color, iter, st);
+    return mand ? sweep_impl<31, true>(a, color, iter, st) : sweep_impl<31, false>(a, color, iter, st);
+}
+
+cudaError_t launch_export(const RunArgs& a, cudaStream_t st) {
+    dim3 block(32, 8), grid((a.W + 31) / 32, (a.H + 7) / 8);
+    k_export<<<grid, block, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eval_costs(const RunArgs& a, int n, const int32_t* px, const float4* planes, float* out,
+                              cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_eval_costs<<<(n + 127) / 128, 128, 0, st>>>(a, n, px, planes, out);
+    return cudaGetLastError();
+}
+
+}  // namespace hpm

@@ -1,0 +1,54 @@
+// PatchMatch run arguments and kernel declarations shared by pm_kernels.cu and
+// the host-side launcher.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "hpm_types.h"
+
+namespace hpm {
+
+struct ViewPoseH {  // host mirror of ViewPose (same layout)
+    float Rr[9];
+    float tr[3];
+};
+
+// Everything one PatchMatch run of one reference view reads.  Passed by value
+// as a __grid_constant__ kernel parameter (about 6 KB).
+struct RunArgs {
+    hpm_camera cams[32];            // 0 = reference
+    ViewPoseH pose[32];             // relative pose of source j+1 w.r.t. the reference
+    cudaTextureObject_t tex[32];    // linear-filtered source images (index j+1)
+    const float* depth_src[32];     // geometric mode: source depth maps (index j+1)
+    int dsw[32], dsh[32];           // their sizes
+    const float* ref_img;           // reference grey image (row-major float)
+    float4* planes;                 // per-pixel plane hypothesis (n, w)
+    float* costs;
+    float* pre_costs;
+    uint32_t* sel;                  // selected-view bitmask
+    uint32_t* rng;                  // per-pixel draw counter
+    const float4* prior;            // prior planes (prior mode)
+    const uint8_t* pmask;           // prior plane mask (prior mode)
+    float* conf;                    // confidences (prior / mandatory)
+    const uint8_t* canny;           // 0/255 edge map
+    float* texture;                 // edge-density output
+    const float4* scaled;           // hierarchy input map (scaled_cols x scaled_rows)
+    hpm_params prm;
+    int S, W, H, cover_pairs;
+    uint64_t seed;
+    uint32_t view_id;
+};
+
+// Host launchers (pm_kernels.cu).  Return cudaError_t of the launch.
+cudaError_t launch_random_init(const RunArgs& a, cudaStream_t st);
+cudaError_t launch_half_sweep(const RunArgs& a, int color, int iter, cudaStream_t st);
+cudaError_t launch_export(const RunArgs& a, cudaStream_t st);
+// Fixed-hypothesis costs: out[k*S + j] for pixels px[2k], px[2k+1] and planes[k].
+cudaError_t launch_eval_costs(const RunArgs& a, int n, const int32_t* px, const float4* planes, float* out,
+                              cudaStream_t st);
+
+// Rows covered by the checkerboard launch of RunPatchMatch (HPM.cu:3004-3011):
+// the grid spans ceil(floor(H/2)/16)*16 row pairs.
+inline int covered_row_pairs(int H) { return ((H / 2 + 15) / 16) * 16; }
+
+}  // namespace hpm
