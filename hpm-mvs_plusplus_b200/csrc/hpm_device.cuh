@@ -1,17 +1,15 @@
-// Device-side building blocks of the PatchMatch hot path (sm_100a).
-//
-// The formulas restate HPM-MVS++'s device helpers (HPM.cu:114-564); the
-// structure is new: the reference patch of a pixel (36 texels and their
-// bilateral weights, which do not depend on the hypothesis or the source view)
-// is computed once per pixel per launch and kept in shared memory, so one
-// bilateral NCC costs 36 filtered source fetches plus the moments of the source
-// samples only.
+// Device-side building blocks of the PatchMatch hot path (sm_100a): camera and
+// plane geometry, random plane generation on the counter-based stream, the
+// geometric-consistency cost and the edge-density term.  The formulas restate
+// HPM-MVS++'s device helpers (HPM.cu:114-564) under the rounding conventions of
+// include/hpm_fp.h.
 #pragma once
 
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "hpm_types.h"
 #include "hpm_philox.h"
+#include "hpm_fp.h"
 
 namespace hpm {
 
@@ -82,7 +80,7 @@ __device__ __forceinline__ float4 view_direction(const hpm_camera& c, int px, in
 }
 
 __device__ __forceinline__ void normalize3(float4& v) {
-    const float inv = rsqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+    const float inv = 1.0f / sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
     v.x *= inv; v.y *= inv; v.z *= inv;
 }
 
@@ -110,14 +108,15 @@ __device__ __forceinline__ float4 perturbed_normal(const hpm_camera& c, int px, 
     const float a1 = (rng.uniform() - 0.5f) * perturbation;
     const float a2 = (rng.uniform() - 0.5f) * perturbation;
     const float a3 = (rng.uniform() - 0.5f) * perturbation;
-    float s1, c1, s2, c2, s3, c3;
-    sincosf(a1, &s1, &c1);
-    sincosf(a2, &s2, &c2);
-    sincosf(a3, &s3, &c3);
+    const float s1 = hpm_sinf(a1), s2 = hpm_sinf(a2), s3 = hpm_sinf(a3);
+    const float c1 = hpm_cosf(a1), c2 = hpm_cosf(a2), c3 = hpm_cosf(a3);
+    const float R0 = c2 * c3, R1 = c3 * s1 * s2 - c1 * s3, R2 = s1 * s3 + c1 * c3 * s2;
+    const float R3 = c2 * s3, R4 = c1 * c3 + s1 * s2 * s3, R5 = c1 * s2 * s3 - c3 * s1;
+    const float R6 = -s2, R7 = c2 * s1, R8 = c1 * c2;
     float4 np;
-    np.x = (c2 * c3) * normal.x + (c3 * s1 * s2 - c1 * s3) * normal.y + (s1 * s3 + c1 * c3 * s2) * normal.z;
-    np.y = (c2 * s3) * normal.x + (c1 * c3 + s1 * s2 * s3) * normal.y + (c1 * s2 * s3 - c3 * s1) * normal.z;
-    np.z = (-s2) * normal.x + (c2 * s1) * normal.y + (c1 * c2) * normal.z;
+    np.x = R0 * normal.x + R1 * normal.y + R2 * normal.z;
+    np.y = R3 * normal.x + R4 * normal.y + R5 * normal.z;
+    np.z = R6 * normal.x + R7 * normal.y + R8 * normal.z;
     np.w = normal.w;
     if (np.x * vd.x + np.y * vd.y + np.z * vd.z >= 0.0f) np = normal;
     normalize3(np);
@@ -234,96 +233,6 @@ __device__ __forceinline__ float texture_term(const uint8_t* __restrict__ canny,
         }
     const float frac = edges * 1.0f / total;
     return (float)(((double)frac + 0.00005) / ((double)frac + 0.0001));
-}
-
-// Statistics of a pixel's reference patch (view-independent part of the NCC).
-struct RefStats {
-    float mean;      // sum_ref / weight_sum
-    float var;       // reference variance
-    float inv_w;     // 1 / weight_sum
-};
-
-// Loads the reference patch of (px, py) into per-thread shared-memory slots
-// patch[k * stride] = (w_k, w_k * r_k) and returns its statistics.  The weights
-// follow ComputeBilateralWeight (HPM.cu:342-347): unsquared spatial distance and
-// unsquared colour distance over 2*sigma^2.
-__device__ __forceinline__ RefStats load_ref_patch(const float* __restrict__ ref, int W, int H, int px, int py,
-                                                   float sigma_spatial, float sigma_color,
-                                                   float2* patch, int stride) {
-    const float center = __ldg(ref + (size_t)clampi(py, 0, H - 1) * W + clampi(px, 0, W - 1));
-    const float two_ss = 2.0f * sigma_spatial * sigma_spatial;
-    const float two_sc = 2.0f * sigma_color * sigma_color;
-    float s_r = 0.f, s_rr = 0.f, s_w = 0.f;
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        float r_r = 0.f, r_rr = 0.f, r_w = 0.f;
-        const int dx = -kPatchRadius + kPatchStep * i;
-        const int x = clampi(px + dx, 0, W - 1);
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-            const int dy = -kPatchRadius + kPatchStep * j;
-            const float r = __ldg(ref + (size_t)clampi(py + dy, 0, H - 1) * W + x);
-            const float sd = sqrtf((float)(dx * dx + dy * dy));
-            const float w = __expf(-sd / two_ss - fabsf(r - center) / two_sc);
-            const float wr = w * r;
-            patch[(i * 6 + j) * stride] = make_float2(w, wr);
-            r_r += wr;
-            r_rr += wr * r;
-            r_w += w;
-        }
-        s_r += r_r; s_rr += r_rr; s_w += r_w;
-    }
-    RefStats st;
-    st.inv_w = 1.0f / s_w;
-    st.mean = s_r * st.inv_w;
-    st.var = s_rr * st.inv_w - st.mean * st.mean;
-    return st;
-}
-
-// Bilateral NCC of one (pixel, plane, source view) (HPM.cu:375-448) sampling the
-// source through the texture unit (linear filter, clamp).
-__device__ __forceinline__ float ncc_tex(cudaTextureObject_t src, int sw, int sh, const float H[9], int px, int py,
-                                         const RefStats& rs, const float2* patch, int stride) {
-    const float cost_max = 2.0f;
-    {
-        const float cx = H[0] * px + H[1] * py + H[2];
-        const float cy = H[3] * px + H[4] * py + H[5];
-        const float cz = H[6] * px + H[7] * py + H[8];
-        const float ux = cx / cz, uy = cy / cz;
-        if (ux >= sw || ux < 0.0f || uy >= sh || uy < 0.0f) return cost_max;
-    }
-    float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        const int x = px - kPatchRadius + kPatchStep * i;
-        float r_s = 0.f, r_ss = 0.f, r_rs = 0.f;
-        float vals[6];
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-            const int y = py - kPatchRadius + kPatchStep * j;
-            const float qx = H[0] * x + H[1] * y + H[2];
-            const float qy = H[3] * x + H[4] * y + H[5];
-            const float qz = H[6] * x + H[7] * y + H[8];
-            vals[j] = tex2D<float>(src, qx / qz + 0.5f, qy / qz + 0.5f);
-        }
-#pragma unroll
-        for (int j = 0; j < 6; ++j) {
-            const float2 wr = patch[(i * 6 + j) * stride];
-            const float s = vals[j];
-            const float ws = wr.x * s;
-            r_s += ws;
-            r_ss += ws * s;
-            r_rs += wr.y * s;
-        }
-        s_s += r_s; s_ss += r_ss; s_rs += r_rs;
-    }
-    s_s *= rs.inv_w; s_ss *= rs.inv_w; s_rs *= rs.inv_w;
-    const float var_s = s_ss - s_s * s_s;
-    const float kMinVar = 1e-5f;
-    if (rs.var < kMinVar || var_s < kMinVar) return cost_max;
-    const float cov = s_rs - rs.mean * s_s;
-    const float vrs = sqrtf(rs.var * var_s);
-    return fmaxf(0.0f, fminf(cost_max, 1.0f - cov / vrs));
 }
 
 }  // namespace hpm

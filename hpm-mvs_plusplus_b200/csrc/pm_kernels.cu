@@ -15,7 +15,9 @@
 //     zero weight is exactly 0 because the NCC is never NaN), and a reference
 //     patch with variance < 1e-5 yields cost 2 for every hypothesis without
 //     sampling (exactly the reference's result).
-// Compiled with --use_fast_math like the reference (CMakeLists.txt:10).
+// Arithmetic follows include/hpm_fp.h (IEEE fp32, explicit fused multiply-adds),
+// which the CPU oracle shares, so the two differ only where the texture unit's
+// filtered sample does (about 0.6 % of samples, by one ulp).
 #include "hpm_device.cuh"
 #include "pm_kernels.cuh"
 
@@ -35,8 +37,15 @@ struct Scratch {
     __device__ __forceinline__ int& pos(int d) const { return reinterpret_cast<int*>(base)[(9 * NS + 8 + d) * BLK]; }
 };
 
+// Statistics of a pixel's reference patch (the view-independent part of the NCC).
+struct RefStats {
+    float mean;   // sum_ref / weight_sum
+    float var;    // reference variance
+    float inv_w;  // 1 / weight_sum
+};
+
 struct Patch {
-    float2 p[kPatchSamples];
+    float2 p[kPatchSamples];  // (w_k, w_k * r_k)
     RefStats rs;
 };
 
@@ -57,11 +66,11 @@ __device__ __forceinline__ void build_patch(const RunArgs& a, int px, int py, Pa
             const int dy = -kPatchRadius + kPatchStep * j;
             const float r = __ldg(ref + (size_t)clampi(py + dy, 0, H - 1) * W + x);
             const float sd = sqrtf((float)(dx * dx + dy * dy));
-            const float w = __expf(-sd / two_ss - fabsf(r - center) / two_sc);
+            const float w = hpm_expf(-sd / two_ss - fabsf(r - center) / two_sc);
             const float wr = w * r;
             P.p[i * 6 + j] = make_float2(w, wr);
             r_r += wr;
-            r_rr += wr * r;
+            r_rr = hpm_fma(wr, r, r_rr);
             r_w += w;
         }
         s_r += r_r; s_rr += r_rr; s_w += r_w;
@@ -80,26 +89,30 @@ __device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int 
     float H[9];
     plane_homography(rc, sc, reinterpret_cast<const ViewPose&>(a.pose[j + 1]), pl, H);
     const int sw = sc.width, sh = sc.height;
+    float iz_c;
     {
-        const float cx = H[0] * px + H[1] * py + H[2];
-        const float cy = H[3] * px + H[4] * py + H[5];
-        const float cz = H[6] * px + H[7] * py + H[8];
-        const float ux = cx / cz, uy = cy / cz;
+        const float fx = (float)px, fy = (float)py;
+        const float cx = hpm_fma(H[0], fx, hpm_fma(H[1], fy, H[2]));
+        const float cy = hpm_fma(H[3], fx, hpm_fma(H[4], fy, H[5]));
+        const float cz = hpm_fma(H[6], fx, hpm_fma(H[7], fy, H[8]));
+        iz_c = 1.0f / cz;
+        const float ux = cx * iz_c, uy = cy * iz_c;
         if (ux >= sw || ux < 0.0f || uy >= sh || uy < 0.0f) return cost_max;
     }
     const cudaTextureObject_t tex = a.tex[j + 1];
     float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        const int x = px - kPatchRadius + kPatchStep * i;
+        const float x = (float)(px - kPatchRadius + kPatchStep * i);
         float v[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            const int y = py - kPatchRadius + kPatchStep * k;
-            const float qx = H[0] * x + H[1] * y + H[2];
-            const float qy = H[3] * x + H[4] * y + H[5];
-            const float qz = H[6] * x + H[7] * y + H[8];
-            v[k] = tex2D<float>(tex, qx / qz + 0.5f, qy / qz + 0.5f);
+            const float y = (float)(py - kPatchRadius + kPatchStep * k);
+            const float qx = hpm_fma(H[0], x, hpm_fma(H[1], y, H[2]));
+            const float qy = hpm_fma(H[3], x, hpm_fma(H[4], y, H[5]));
+            const float qz = hpm_fma(H[6], x, hpm_fma(H[7], y, H[8]));
+            const float iz = hpm_recip_near(qz, iz_c);
+            v[k] = tex2D<float>(tex, hpm_fma(qx, iz, 0.5f), hpm_fma(qy, iz, 0.5f));
         }
         float r_s = 0.f, r_ss = 0.f, r_rs = 0.f;
 #pragma unroll
@@ -107,8 +120,8 @@ __device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int 
             const float2 w = P.p[i * 6 + k];
             const float ws = w.x * v[k];
             r_s += ws;
-            r_ss += ws * v[k];
-            r_rs += w.y * v[k];
+            r_ss = hpm_fma(ws, v[k], r_ss);
+            r_rs = hpm_fma(w.y, v[k], r_rs);
         }
         s_s += r_s; s_ss += r_ss; s_rs += r_rs;
     }
@@ -425,7 +438,7 @@ __device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, 
                 if (j < S) priors[j] += ((m >> j) & 1u) ? 0.9f : 0.1f;
         }
     }
-    const float cost_thr = (float)(0.8 * __expf((float)(iter * iter) / (-90.0f)));
+    const float cost_thr = (float)(0.8 * hpm_expf((float)(iter * iter) / (-90.0f)));
     float probs[NS];
 #pragma unroll
     for (int j = 0; j < NS; ++j) {
@@ -436,11 +449,11 @@ __device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, 
 #pragma unroll
             for (int d = 0; d < 8; ++d) {
                 const float c = s.ca(d, j);
-                if (c < cost_thr) { tmpw += __expf(c * c / (-0.18f)); count += 1.0f; }
+                if (c < cost_thr) { tmpw += hpm_expf(c * c / (-0.18f)); count += 1.0f; }
                 if (c > 1.2f) ++count_false;
             }
             if (count > 2 && count_false < 3) probs[j] = tmpw / count;
-            else if (count_false < 3) probs[j] = __expf(cost_thr * cost_thr / (-0.32f));
+            else if (count_false < 3) probs[j] = hpm_expf(cost_thr * cost_thr / (-0.32f));
             probs[j] = probs[j] * priors[j];
         }
     }
@@ -534,7 +547,7 @@ __device__ __forceinline__ float prior_score(float final_cost, float depth_now, 
     const float gamma = 0.5f, beta = 0.18f;
     const float dd = depth_now - depth_prior;
     const float nd = fabsf(pp.x - pl.x) + fabsf(pp.y - pl.y) + fabsf(pp.z - pl.z);
-    const float prior = (float)(gamma * (1.2 - 0.2 * texture) + (double)(__expf(-dd * dd / two_dss) * __expf(-nd * nd / two_ass)));
+    const float prior = (float)(gamma * (1.2 - 0.2 * texture) + (double)(hpm_expf(-dd * dd / two_dss) * hpm_expf(-nd * nd / two_ass)));
     return (float)(exp(-final_cost * final_cost / beta * (1 + 0.2 * texture)) * (double)prior);
 }
 
@@ -715,11 +728,11 @@ __global__ void __launch_bounds__(BLK) k_half_sweep(const __grid_constant__ RunA
             rfc[d] = 0.0f;
             if (o.flags & (1u << d)) {
                 const float cp = a.conf[s.pos(d)];
-                const float gce = __expf(-fcl[d] * fcl[d] / beta);
+                const float gce = hpm_expf(-fcl[d] * fcl[d] / beta);
                 const float dm = fmaxf(0.0f, mmc - cp);
                 const float mce = (float)(0.5f + exp(-dm * dm / (mmc * mmc * 1.0)));
                 rfc[d] = (cp > 0) ? fmaxf(3.0f, mce) * gce : mce * gce;
-                if (cp > 0) fcl[d] = (float)(fcl[d] * fmin((double)__expf(-cp * 2), 0.35));
+                if (cp > 0) fcl[d] = (float)(fcl[d] * fmin((double)hpm_expf(-cp * 2), 0.35));
             }
         }
         const int max_idx = find_max_index8(rfc);
@@ -727,12 +740,12 @@ __global__ void __launch_bounds__(BLK) k_half_sweep(const __grid_constant__ RunA
         float cost_now = selected_cost(a, P, px, py, cur, o.temp_selected, o.weight_norm, s);
         const float cost_chk = cost_now;
         const float cc = a.conf[center];
-        const float gce = __expf(-cost_now * cost_now / beta);
+        const float gce = hpm_expf(-cost_now * cost_now / beta);
         const float dm = fmaxf(0.0f, mmc - cc);
         const float mce = (float)(0.5f + exp(-dm * dm / (mmc * mmc * 1.0)));
         const float rnow = (cc > 0) ? fmaxf(3.0f, mce) * gce : mce * gce;
         if (cc < 0.3) cost_now = (float)(cost_now * exp(0.2 + cc * 2));
-        else cost_now = cost_now * __expf(-cc * 2);
+        else cost_now = cost_now * hpm_expf(-cc * 2);
         float4 plane_now = cur;  // uninitialised in the reference (HPM.cu:2761)
         if (o.flags & (1u << max_idx)) {
             const int pm = s.pos(max_idx);

@@ -13,6 +13,7 @@
  */
 #include "hpm_oracle.h"
 #include "hpm_philox.h"
+#include "hpm_fp.h"
 
 #include <float.h>
 #include <math.h>
@@ -53,34 +54,44 @@ static inline void store4(float *p, int idx, f4 v)
     p[4 * idx] = v.x; p[4 * idx + 1] = v.y; p[4 * idx + 2] = v.z; p[4 * idx + 3] = v.w;
 }
 
-/* Linear-filtered fetch with unnormalised coordinates (CUDA Programming Guide,
- * "Texture Fetching", linear filtering): xB = x - 0.5, i = floor(xB),
- * alpha = frac(xB) held with 8 fractional bits; clamp addressing. */
+/* Linear-filtered fetch with unnormalised coordinates and clamp addressing
+ * (tex2D on a cudaFilterModeLinear float texture, HPM.cu:409).
+ *
+ * Model 0 is the filter as measured on B200 (sm_100a): xB = x - 0.5, i =
+ * floor(xB), and the fractional weights alpha, beta rounded half-up to 8
+ * fractional bits; the cross weight alpha*beta is itself rounded half-up to 8
+ * bits and the other three weights are derived from it so each row and column
+ * still sums exactly.  NaN coordinates read as 0.  Model 1 is the separable
+ * form of the CUDA Programming Guide ("Texture Fetching": 9-bit fixed-point
+ * alpha and beta, products in float). */
 float ora_tex2d(const float *img, int width, int height, float x, float y)
 {
-    if (x != x || y != y) return 0.0f;
-    const double xb = (double)x - 0.5;
-    const double yb = (double)y - 0.5;
-    double fx, fy;
-    if (g_tex_model == 0) { fx = floor(xb * 256.0 + 0.5); fy = floor(yb * 256.0 + 0.5); }
-    else { fx = floor(xb * 256.0); fy = floor(yb * 256.0); }
-    /* clamp far-away coordinates before integer conversion */
+    if (x != x) x = 0.0f;
+    if (y != y) y = 0.0f;
+    double xb = (double)x - 0.5;
+    double yb = (double)y - 0.5;
     const double lim = 1.0e9;
-    if (fx > lim) fx = lim;
-    if (fx < -lim) fx = -lim;
-    if (fy > lim) fy = lim;
-    if (fy < -lim) fy = -lim;
-    const long long ix = (long long)fx, iy = (long long)fy;
-    long long i0 = ix >> 8, j0 = iy >> 8;  /* arithmetic shift = floor division */
-    const float a = (float)(ix & 255) * (1.0f / 256.0f);
-    const float b = (float)(iy & 255) * (1.0f / 256.0f);
+    if (xb > lim) xb = lim;
+    if (xb < -lim) xb = -lim;
+    if (yb > lim) yb = lim;
+    if (yb < -lim) yb = -lim;
+    const long long ix = (long long)floor(xb * 256.0 + 0.5);
+    const long long iy = (long long)floor(yb * 256.0 + 0.5);
+    const long long i0 = ix >> 8, j0 = iy >> 8; /* arithmetic shift = floor division */
+    const int ai = (int)(ix & 255), bi = (int)(iy & 255);
     const int x0 = (int)(i0 < 0 ? 0 : (i0 > width - 1 ? width - 1 : i0));
     const int x1 = (int)(i0 + 1 < 0 ? 0 : (i0 + 1 > width - 1 ? width - 1 : i0 + 1));
     const int y0 = (int)(j0 < 0 ? 0 : (j0 > height - 1 ? height - 1 : j0));
     const int y1 = (int)(j0 + 1 < 0 ? 0 : (j0 + 1 > height - 1 ? height - 1 : j0 + 1));
     const float t00 = img[y0 * width + x0], t10 = img[y0 * width + x1];
     const float t01 = img[y1 * width + x0], t11 = img[y1 * width + x1];
-    return (1.0f - a) * (1.0f - b) * t00 + a * (1.0f - b) * t10 + (1.0f - a) * b * t01 + a * b * t11;
+    const float a = (float)ai * (1.0f / 256.0f);
+    const float b = (float)bi * (1.0f / 256.0f);
+    if (g_tex_model == 1)
+        return (1.0f - a) * (1.0f - b) * t00 + a * (1.0f - b) * t10 + (1.0f - a) * b * t01 + a * b * t11;
+    const float w11 = (float)((ai * bi + 128) >> 8) * (1.0f / 256.0f);
+    const float w10 = a - w11, w01 = b - w11, w00 = 1.0f - a - b + w11;
+    return w00 * t00 + w10 * t10 + w01 * t01 + w11 * t11;
 }
 
 /* Texel fetch at an integer position (tex2D at x + 0.5, y + 0.5), clamped. */
@@ -229,8 +240,8 @@ static f4 perturbed_normal(const hpm_camera *c, int px, int py, f4 normal, rng_t
     const float a1 = (rng_uniform(rng) - 0.5f) * perturbation;
     const float a2 = (rng_uniform(rng) - 0.5f) * perturbation;
     const float a3 = (rng_uniform(rng) - 0.5f) * perturbation;
-    const float s1 = sinf(a1), s2 = sinf(a2), s3 = sinf(a3);
-    const float c1 = cosf(a1), c2 = cosf(a2), c3 = cosf(a3);
+    const float s1 = hpm_sinf(a1), s2 = hpm_sinf(a2), s3 = hpm_sinf(a3);
+    const float c1 = hpm_cosf(a1), c2 = hpm_cosf(a2), c3 = hpm_cosf(a3);
     float R[9];
     R[0] = c2 * c3;
     R[1] = c3 * s1 * s2 - c1 * s3;
@@ -264,50 +275,78 @@ static f4 random_plane(const hpm_camera *c, int px, int py, rng_t *rng, float dm
 float ora_bilateral_ncc(const float *ref, const hpm_camera *rc, const float *src, const hpm_camera *sc,
                         int px, int py, const float plane[4], const hpm_params *prm)
 {
+    /* HPM.cu:375-448.  The reference patch statistics (view independent) are
+     * formed first, then the source moments; both follow include/hpm_fp.h. */
     const float cost_max = 2.0f;
-    const int radius = prm->patch_size / 2;
+    const int rw = rc->width, rh = rc->height, sw = sc->width, sh = sc->height;
+    const float center = texel(ref, rw, rh, px, py);
+    const float two_ss = 2.0f * prm->sigma_spatial * prm->sigma_spatial;
+    const float two_sc = 2.0f * prm->sigma_color * prm->sigma_color;
+    float pw[36], pwr[36];
+    float s_r = 0.f, s_rr = 0.f, s_w = 0.f;
+    for (int i = 0; i < 6; ++i) {
+        float r_r = 0.f, r_rr = 0.f, r_w = 0.f;
+        const int dx = -5 + 2 * i;
+        for (int j = 0; j < 6; ++j) {
+            const int dy = -5 + 2 * j;
+            const float r = texel(ref, rw, rh, px + dx, py + dy);
+            const float sd = sqrtf((float)(dx * dx + dy * dy));
+            const float w = hpm_expf(-sd / two_ss - fabsf(r - center) / two_sc);
+            const float wr = w * r;
+            pw[i * 6 + j] = w;
+            pwr[i * 6 + j] = wr;
+            r_r += wr;
+            r_rr = hpm_fma(wr, r, r_rr);
+            r_w += w;
+        }
+        s_r += r_r; s_rr += r_rr; s_w += r_w;
+    }
+    const float inv_w = 1.0f / s_w;
+    const float mean_r = s_r * inv_w;
+    const float var_r = s_rr * inv_w - mean_r * mean_r;
+    const float kMinVar = 1e-5f;
+    if (var_r < kMinVar) return cost_max;
+
     const f4 pl = { plane[0], plane[1], plane[2], plane[3] };
     float H[9];
     homography(rc, sc, pl, H);
-    const f2 pt = corresponding_point(H, px, py);
-    if (pt.x >= sc->width || pt.x < 0.0f || pt.y >= sc->height || pt.y < 0.0f) return cost_max;
-
-    const int rw = rc->width, rh = rc->height, sw = sc->width, sh = sc->height;
-    float s_r = 0, s_rr = 0, s_s = 0, s_ss = 0, s_rs = 0, s_w = 0;
-    const float rc_pix = texel(ref, rw, rh, px, py);
-    const float two_ss = 2.0f * prm->sigma_spatial * prm->sigma_spatial;
-    const float two_sc = 2.0f * prm->sigma_color * prm->sigma_color;
-    for (int i = -radius; i < radius + 1; i += prm->radius_increment) {
-        float r_r = 0, r_s = 0, r_rr = 0, r_ss = 0, r_rs = 0, r_w = 0;
-        for (int j = -radius; j < radius + 1; j += prm->radius_increment) {
-            const int rx = px + i, ry = py + j;
-            const float rpix = texel(ref, rw, rh, rx, ry);
-            const f2 sp = corresponding_point(H, rx, ry);
-            const float spix = ora_tex2d(src, sw, sh, sp.x + 0.5f, sp.y + 0.5f);
-            const float sd = sqrtf((float)i * (float)i + (float)j * (float)j);
-            const float cd = fabsf(rpix - rc_pix);
-            const float w = expf(-sd / two_ss - cd / two_sc);
-            r_r += w * rpix;
-            r_rr += w * rpix * rpix;
-            r_s += w * spix;
-            r_ss += w * spix * spix;
-            r_rs += w * rpix * spix;
-            r_w += w;
-        }
-        s_r += r_r; s_rr += r_rr; s_s += r_s; s_ss += r_ss; s_rs += r_rs; s_w += r_w;
+    float iz_c;
+    {
+        const float fx = (float)px, fy = (float)py;
+        const float cx = hpm_fma(H[0], fx, hpm_fma(H[1], fy, H[2]));
+        const float cy = hpm_fma(H[3], fx, hpm_fma(H[4], fy, H[5]));
+        const float cz = hpm_fma(H[6], fx, hpm_fma(H[7], fy, H[8]));
+        iz_c = 1.0f / cz;
+        const float ux = cx * iz_c, uy = cy * iz_c;
+        if (ux >= sw || ux < 0.0f || uy >= sh || uy < 0.0f) return cost_max;
     }
-    const float inv = 1.0f / s_w;
-    s_r *= inv; s_rr *= inv; s_s *= inv; s_ss *= inv; s_rs *= inv;
-    const float var_r = s_rr - s_r * s_r;
+    float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
+    for (int i = 0; i < 6; ++i) {
+        const float x = (float)(px - 5 + 2 * i);
+        float r_s = 0.f, r_ss = 0.f, r_rs = 0.f;
+        for (int k = 0; k < 6; ++k) {
+            const float y = (float)(py - 5 + 2 * k);
+            const float qx = hpm_fma(H[0], x, hpm_fma(H[1], y, H[2]));
+            const float qy = hpm_fma(H[3], x, hpm_fma(H[4], y, H[5]));
+            const float qz = hpm_fma(H[6], x, hpm_fma(H[7], y, H[8]));
+            const float iz = hpm_recip_near(qz, iz_c);
+            const float v = ora_tex2d(src, sw, sh, hpm_fma(qx, iz, 0.5f), hpm_fma(qy, iz, 0.5f));
+            const float ws = pw[i * 6 + k] * v;
+            r_s += ws;
+            r_ss = hpm_fma(ws, v, r_ss);
+            r_rs = hpm_fma(pwr[i * 6 + k], v, r_rs);
+        }
+        s_s += r_s; s_ss += r_ss; s_rs += r_rs;
+    }
+    s_s *= inv_w; s_ss *= inv_w; s_rs *= inv_w;
     const float var_s = s_ss - s_s * s_s;
-    const float kMinVar = 1e-5f;
-    if (var_r < kMinVar || var_s < kMinVar) return cost_max;
-    const float cov = s_rs - s_r * s_s;
+    if (var_s < kMinVar) return cost_max;
+    const float cov = s_rs - mean_r * s_s;
     const float vrs = sqrtf(var_r * var_s);
     float c = 1.0f - cov / vrs;
-    /* max(0, min(2, c)) with CUDA fminf/fmaxf NaN semantics */
-    c = (c < cost_max || c != c) ? (c != c ? cost_max : c) : cost_max;
-    c = c > 0.0f ? c : 0.0f;
+    /* max(0, min(2, c)) with fminf/fmaxf NaN semantics (the non-NaN operand wins) */
+    c = fminf(cost_max, c);
+    c = fmaxf(0.0f, c);
     return c;
 }
 
@@ -620,7 +659,7 @@ static float prior_score(float final_cost, float depth_now, float depth_prior, f
     const float gamma = 0.5f, beta = 0.18f;
     const float dd = depth_now - depth_prior;
     const float nd = fabsf(prior_pl.x - pl.x) + fabsf(prior_pl.y - pl.y) + fabsf(prior_pl.z - pl.z);
-    const float prior = (float)(gamma * (1.2 - 0.2 * texture) + (double)(expf(-dd * dd / two_dss) * expf(-nd * nd / two_ass)));
+    const float prior = (float)(gamma * (1.2 - 0.2 * texture) + (double)(hpm_expf(-dd * dd / two_dss) * hpm_expf(-nd * nd / two_ass)));
     return (float)(exp(-final_cost * final_cost / beta * (1 + 0.2 * texture)) * (double)prior);
 }
 
@@ -806,16 +845,16 @@ static void propagate_common(const float *const *images, const float *const *dep
             }
     float probs[32];
     for (int j = 0; j < 32; ++j) probs[j] = 0.0f;
-    const float cost_thr = (float)(0.8 * expf((float)(iter * iter) / (-90.0f)));
+    const float cost_thr = (float)(0.8 * hpm_expf((float)(iter * iter) / (-90.0f)));
     for (int i = 0; i < S; ++i) {
         float count = 0; int count_false = 0; float tmpw = 0;
         for (int j = 0; j < 8; ++j) {
             const float c = s->cost_array[j][i];
-            if (c < cost_thr) { tmpw += expf(c * c / (-0.18f)); count++; }
+            if (c < cost_thr) { tmpw += hpm_expf(c * c / (-0.18f)); count++; }
             if (c > 1.2f) count_false++;
         }
         if (count > 2 && count_false < 3) probs[i] = tmpw / count;
-        else if (count_false < 3) probs[i] = expf(cost_thr * cost_thr / (-0.32f));
+        else if (count_false < 3) probs[i] = hpm_expf(cost_thr * cost_thr / (-0.32f));
         probs[i] = probs[i] * priors[i];
     }
     /* TransformPDFToCDF (HPM.cu:98-112) */
@@ -1010,13 +1049,13 @@ static void propagate_pixel_mand(const float *const *images, const float *const 
     for (int i = 0; i < 8; ++i) {
         if (s.flag[i]) {
             const float cp = st->confidences[s.positions[i]];
-            const float gce = expf(-s.final_costs[i] * s.final_costs[i] / beta);
+            const float gce = hpm_expf(-s.final_costs[i] * s.final_costs[i] / beta);
             const float dm = (0.0f > mmc - cp) ? 0.0f : (mmc - cp);
             const float mce = (float)(0.5f + exp(-dm * dm / (mmc * mmc * 1.0)));
             if (cp > 0) rfc[i] = (3.0f > mce ? 3.0f : mce) * gce;
             else rfc[i] = mce * gce;
             if (cp > 0) {
-                const double e = (double)expf(-cp * 2);
+                const double e = (double)hpm_expf(-cp * 2);
                 s.final_costs[i] = (float)(s.final_costs[i] * (e < 0.35 ? e : 0.35));
             }
         }
@@ -1026,14 +1065,14 @@ static void propagate_pixel_mand(const float *const *images, const float *const 
                                   s.view_weights, s.weight_norm);
     st->costs[center] = cost_now;
     const float cc = st->confidences[center];
-    const float gce = expf(-cost_now * cost_now / beta);
+    const float gce = hpm_expf(-cost_now * cost_now / beta);
     const float dm = (0.0f > mmc - cc) ? 0.0f : (mmc - cc);
     const float mce = (float)(0.5f + exp(-dm * dm / (mmc * mmc * 1.0)));
     float rnow;
     if (cc > 0) rnow = (3.0f > mce ? 3.0f : mce) * gce;
     else rnow = mce * gce;
     if (cc < 0.3) cost_now = (float)(cost_now * exp(0.2 + cc * 2));
-    else cost_now = cost_now * expf(-cc * 2);
+    else cost_now = cost_now * hpm_expf(-cc * 2);
 
     f4 plane_now = load4(st->planes, center); /* defined value for HPM.cu:2761 */
     if (s.flag[max_idx]) {

@@ -19,7 +19,7 @@ def declared_functions() -> list[str]:
         text = open(hdr).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"^([A-Za-z_][\w \*]*?)\b(hpm_\w+)\s*\(", text, flags=re.M):
-            if m.group(1).strip().startswith(("HPM_HD", "static")):
+            if m.group(1).strip().startswith(("HPM_HD", "HPM_FP_HD", "static")):
                 continue  # header-only inline helpers, not library symbols
             names.append(m.group(2))
     return sorted(set(names))
