@@ -39,8 +39,15 @@ MAP_TEXTURE0 = 8
 EXPORTED_SYMBOLS = (
     "hpm_create", "hpm_destroy", "hpm_last_error", "hpm_set_view", "hpm_set_map", "hpm_get_map",
     "hpm_set_canny", "hpm_set_prior", "hpm_run_patchmatch", "hpm_eval_costs", "hpm_set_address_mode",
-    "hpm_launch_count", "hpm_synchronize", "hpm_sample_view", "hpm_debug_run_partial",
+    "hpm_launch_count", "hpm_synchronize", "hpm_sample_view", "hpm_debug_run_partial", "hpm_set_color",
+    "hpm_jbu", "hpm_jbu_maps", "hpm_confidence_eval", "hpm_fuse",
 )
+
+
+class Point(ctypes.Structure):
+    """hpm_point == PointList (main.h:92-96): world xyz, world normal, BGR colour."""
+
+    _fields_ = [("coord", ctypes.c_float * 3), ("normal", ctypes.c_float * 3), ("color", ctypes.c_float * 3)]
 
 
 class Camera(ctypes.Structure):
@@ -160,6 +167,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.hpm_launch_count.restype = ctypes.c_int64
     lib.hpm_synchronize.argtypes = [vp]
     lib.hpm_sample_view.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
+    lib.hpm_set_color.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int]
+    lib.hpm_jbu.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.hpm_jbu_maps.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
+    lib.hpm_confidence_eval.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.hpm_fuse.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, ctypes.c_int64,
+                             ctypes.POINTER(ctypes.c_int64)]
     lib.hpm_debug_run_partial.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int,
                                           ctypes.c_uint64, ctypes.c_int, vp, vp, vp, vp]
     for name in EXPORTED_SYMBOLS:
@@ -275,6 +288,60 @@ class Context:
                                                    ctypes.c_uint64(seed), n_half_sweeps, _ptr(planes), _ptr(costs),
                                                    _ptr(sel), _ptr(draws)), "hpm_debug_run_partial")
         return {"planes": planes, "costs": costs, "selected_views": sel, "rng_draw": draws}
+
+    def set_color(self, view: int, bgr: np.ndarray) -> None:
+        c = np.ascontiguousarray(bgr, dtype=np.uint8)
+        h, w = c.shape[:2]
+        self._check(self.lib.hpm_set_color(self.h, view, _ptr(c), w, h), "hpm_set_color")
+
+    def jbu(self, view: int) -> bool:
+        applied = ctypes.c_int()
+        self._check(self.lib.hpm_jbu(self.h, view, ctypes.byref(applied)), "hpm_jbu")
+        return bool(applied.value)
+
+    def jbu_maps(self, view: int, src_depth: np.ndarray, src_normal: np.ndarray | None = None):
+        sd = np.ascontiguousarray(src_depth, np.float32)
+        sn = None if src_normal is None else np.ascontiguousarray(src_normal, np.float32)
+        w, h = self.views[view]
+        od = np.empty((h, w), np.float32)
+        on = None if sn is None else np.empty((h, w, 3), np.float32)
+        self._check(self.lib.hpm_jbu_maps(self.h, view, _ptr(sd), None if sn is None else _ptr(sn), sd.shape[1],
+                                          sd.shape[0], _ptr(od), None if on is None else _ptr(on)), "hpm_jbu_maps")
+        return od if on is None else (od, on)
+
+    @staticmethod
+    def _src_lists(src_lists):
+        off = np.zeros(len(src_lists) + 1, np.int32)
+        for i, s in enumerate(src_lists):
+            off[i + 1] = off[i] + len(s)
+        ids = np.ascontiguousarray(np.concatenate([np.asarray(s, np.int32) for s in src_lists])
+                                   if off[-1] else np.zeros(1, np.int32), np.int32)
+        return off, ids
+
+    def confidence_eval(self, src_lists, depth_kind: int = MAP_DEPTH) -> int:
+        off, ids = self._src_lists(src_lists)
+        it = ctypes.c_int()
+        self._check(self.lib.hpm_confidence_eval(self.h, len(src_lists), _ptr(off), _ptr(ids), depth_kind,
+                                                 ctypes.byref(it)), "hpm_confidence_eval")
+        return it.value
+
+    def fuse(self, src_lists, depth_kind: int = MAP_DEPTH_GEOM, sky_masks=None, capacity: int | None = None):
+        off, ids = self._src_lists(src_lists)
+        if capacity is None:
+            capacity = sum(w * h for (w, h) in (self.views[v] for v in range(len(src_lists))))
+        out = np.zeros((capacity, 9), np.float32)
+        n = ctypes.c_int64()
+        sky_arr = None
+        keep = []
+        if sky_masks is not None:
+            sky_arr = (ctypes.c_void_p * len(sky_masks))()
+            for i, m in enumerate(sky_masks):
+                m = np.ascontiguousarray(m, np.uint8)
+                keep.append(m)
+                sky_arr[i] = m.ctypes.data
+        self._check(self.lib.hpm_fuse(self.h, len(src_lists), _ptr(off), _ptr(ids), depth_kind, sky_arr, _ptr(out),
+                                      capacity, ctypes.byref(n)), "hpm_fuse")
+        return out[: min(n.value, capacity)], n.value
 
     def synchronize(self) -> None:
         self._check(self.lib.hpm_synchronize(self.h), "hpm_synchronize")

@@ -4,6 +4,7 @@
 #include "hpm_capi.h"
 #include "ctx.hpp"
 #include "pm_kernels.cuh"
+#include "aux_kernels.cuh"
 
 #include <algorithm>
 #include <cstdarg>
@@ -26,6 +27,7 @@ int Ctx::fail(int code, const char* fmt, ...) {
 }
 
 int Ctx::cuda_fail(cudaError_t e, const char* what) {
+    cudaGetLastError();  // clear the runtime's last-error state so the next launch check is not stale
     return fail(HPM_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
@@ -68,9 +70,10 @@ Ctx::~Ctx() {
         if (v.canny) cudaFree(v.canny);
         if (v.prior) cudaFree(v.prior);
         if (v.pmask) cudaFree(v.pmask);
+        if (v.color) cudaFree(v.color);
     }
     for (void* p : { (void*)planes, (void*)costs, (void*)pre_costs, (void*)sel, (void*)rng, (void*)conf,
-                     (void*)scaled, (void*)scratch })
+                     (void*)scaled, (void*)scratch, (void*)scan_state, (void*)scan_work, (void*)points })
         if (p) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -276,6 +279,87 @@ int hpm_eval_costs(hpm_ctx* ctx, int ref, const int32_t* srcs, int n_src, const 
     if (!ctx) return HPM_E_INVALID;
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     return c->eval_costs(ref, srcs, n_src, params, n, px, planes, out);
+}
+
+int hpm_set_color(hpm_ctx* ctx, int view, const uint8_t* bgr, int w, int h) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || !bgr || w <= 0 || h <= 0)
+        return c->fail(HPM_E_INVALID, "hpm_set_color: bad arguments");
+    cudaSetDevice(c->device);
+    ViewState& v = c->views[view];
+    cudaError_t e = ensure(v.color, v.color_cap, (size_t)w * h * 3);
+    if (e != cudaSuccess) return c->cuda_fail(e, "alloc colour");
+    e = cudaMemcpyAsync(v.color, bgr, (size_t)w * h * 3, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "upload colour");
+    v.color_w = w; v.color_h = h;
+    return HPM_OK;
+}
+
+int hpm_jbu(hpm_ctx* ctx, int view, int* applied) {
+    if (!ctx) return HPM_E_INVALID;
+    return reinterpret_cast<Ctx*>(ctx)->jbu_view(view, applied);
+}
+
+int hpm_jbu_maps(hpm_ctx* ctx, int view, const float* src_depth, const float* src_normal, int sw, int sh,
+                 float* out_depth, float* out_normal) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || c->views[view].w == 0) return c->fail(HPM_E_STATE, "view %d not set", view);
+    if (!src_depth || !out_depth || sw <= 0 || sh <= 0 || (src_normal && !out_normal))
+        return c->fail(HPM_E_INVALID, "hpm_jbu_maps: bad arguments");
+    cudaSetDevice(c->device);
+    const ViewState& v = c->views[view];
+    const size_t ns = (size_t)sw * sh, nf = (size_t)v.w * v.h;
+    cudaError_t e = ensure(c->scratch, c->scratch_cap, ns * 16 + nf * 16 + 256);
+    if (e != cudaSuccess) return c->cuda_fail(e, "alloc scratch");
+    float* d_sd = reinterpret_cast<float*>(c->scratch);
+    float* d_sn = d_sd + ns;
+    float* d_od = d_sn + 3 * ns;
+    float* d_on = d_od + nf;
+    e = cudaMemcpyAsync(d_sd, src_depth, 4 * ns, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && src_normal) e = cudaMemcpyAsync(d_sn, src_normal, 12 * ns, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "upload JBU input");
+    e = src_normal ? launch_jbu_prior(v.gray, v.w, v.h, d_sd, d_sn, sw, sh, d_od, d_on, c->stream)
+                   : launch_jbu(v.gray, v.w, v.h, d_sd, sw, sh, d_od, c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "JBU launch");
+    ++c->launches;
+    e = cudaMemcpyAsync(out_depth, d_od, 4 * nf, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && src_normal) e = cudaMemcpyAsync(out_normal, d_on, 12 * nf, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "download JBU output");
+    return HPM_OK;
+}
+
+int hpm_confidence_eval(hpm_ctx* ctx, int n_views, const int32_t* src_off, const int32_t* src_ids, int depth_kind,
+                        int* iterations) {
+    if (!ctx) return HPM_E_INVALID;
+    return reinterpret_cast<Ctx*>(ctx)->consistency_scan(0, n_views, src_off, src_ids, depth_kind, nullptr, nullptr,
+                                                         0, nullptr, iterations);
+}
+
+int hpm_fuse(hpm_ctx* ctx, int n_views, const int32_t* src_off, const int32_t* src_ids, int depth_kind,
+             const uint8_t* const* sky_masks, hpm_point* out, int64_t capacity, int64_t* n_points) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (n_views < 1 || n_views > HPM_MAX_VIEWS) return c->fail(HPM_E_INVALID, "hpm_fuse: bad view count");
+    cudaSetDevice(c->device);
+    size_t total = 0;
+    for (int v = 0; v < n_views; ++v) total += (size_t)c->views[v].maps[depth_kind].w * c->views[v].maps[depth_kind].h;
+    cudaError_t e = ensure(c->points, c->points_cap, total + 1);
+    if (e != cudaSuccess) return c->cuda_fail(e, "alloc points");
+    int64_t n = 0;
+    int rc = c->consistency_scan(1, n_views, src_off, src_ids, depth_kind, sky_masks, c->points, (int64_t)total, &n,
+                                 nullptr);
+    if (rc) return rc;
+    if (n_points) *n_points = n;
+    if (out && capacity > 0) {
+        const int64_t m = n < capacity ? n : capacity;
+        e = cudaMemcpyAsync(out, c->points, sizeof(hpm_point) * (size_t)m, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) return c->cuda_fail(e, "download points");
+    }
+    return HPM_OK;
 }
 
 int hpm_sample_view(hpm_ctx* ctx, int view, int n, const float* xy, float* out) {

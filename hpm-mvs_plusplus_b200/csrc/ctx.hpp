@@ -36,6 +36,9 @@ struct ViewState {
     uint8_t* pmask = nullptr;
     size_t pmask_cap = 0;
     int prior_w = 0, prior_h = 0;
+    uint8_t* color = nullptr;  // BGR at the map size (fusion colours)
+    size_t color_cap = 0;
+    int color_w = 0, color_h = 0;
 };
 
 void compute_pose(const hpm_camera& rc, const hpm_camera& sc, ViewPoseH& vp);
@@ -57,6 +60,9 @@ struct Ctx {
     float* conf = nullptr; size_t run_cap_conf = 0;
     float4* scaled = nullptr; size_t scaled_cap = 0;
     uint8_t* scratch = nullptr; size_t scratch_cap = 0;
+    uint8_t* scan_state = nullptr; size_t scan_state_cap = 0;
+    uint8_t* scan_work = nullptr; size_t scan_work_cap = 0;
+    hpm_point* points = nullptr; size_t points_cap = 0;
 
     ~Ctx();
     int fail(int code, const char* fmt, ...);
@@ -74,6 +80,10 @@ struct Ctx {
     int sample_view(int view, int n, const float* xy, float* out);
     int run_patchmatch(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int texture_level,
                        uint64_t seed);
+    int consistency_scan(int mode, int n_views, const int32_t* src_off, const int32_t* src_ids, int depth_kind,
+                         const uint8_t* const* sky_host, hpm_point* out_device, int64_t capacity, int64_t* n_points,
+                         int* max_iterations_used);
+    int jbu_view(int view, int* applied);
     int eval_costs(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n, const int32_t* px,
                    const float* planes, float* out);
 };

@@ -141,6 +141,7 @@ __device__ float initial_cost(const RunArgs& a, const Patch& P, int px, int py, 
     const float cost_max = 2.0f;
     const int S = a.S;
     int valid = 0;
+#pragma unroll 1
     for (int j = 0; j < S; ++j) {
         const float c = ncc_view(a, P, px, py, pl, j);
         s.ca(0, j) = c;
@@ -297,6 +298,7 @@ __global__ void __launch_bounds__(BLK) k_random_init(const __grid_constant__ Run
 template <int NS, int BLK>
 __device__ __forceinline__ void cost_row(const RunArgs& a, const Patch& P, int px, int py, float4 pl, int d,
                                          const Scratch<NS, BLK>& s) {
+#pragma unroll 1
     for (int j = 0; j < a.S; ++j) s.ca(d, j) = ncc_view(a, P, px, py, pl, j);
 }
 
@@ -391,6 +393,7 @@ __device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, 
 #pragma unroll
     for (int d = 0; d < 8; ++d) s.pos(d) = pos[d];
 
+#pragma unroll 1
     for (int d = 0; d < 8; ++d) {
         if (o.flags & (1u << d)) cost_row(a, P, px, py, a.planes[s.pos(d)], d, s);
     }
@@ -398,6 +401,7 @@ __device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, 
     // Extended propagation: only orientation 0 (left_up) is active because
     // `bool symbol_eight_orientations[10] = { true }` (HPM.cu:1612, 1063-1126).
     if (o.flags & 1u) {
+#pragma unroll 1
         for (int it = 0; it < 3; ++it) {
             const float good_thr = (float)(0.8 * exp(-iter * iter * (3 - it) / 90.0));
             int good = 0, bad = 0;
@@ -487,6 +491,7 @@ __device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, 
             o.num_selected++;
         }
     }
+#pragma unroll 1
     for (int d = 0; d < 8; ++d) {
         float fc = 0.0f;
         const bool valid = o.flags & (1u << d);
@@ -517,6 +522,7 @@ __device__ __forceinline__ float selected_cost(const RunArgs& a, const Patch& P,
                                                uint32_t selmask, float weight_norm, const Scratch<NS, BLK>& s) {
     const bool geom = a.prm.mode & HPM_MODE_GEOM;
     float c = 0.0f;
+#pragma unroll 1
     for (int j = 0; j < a.S; ++j) {
         if (!((selmask >> j) & 1u)) continue;
         const float w = s.vw(j);

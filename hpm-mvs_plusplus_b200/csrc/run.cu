@@ -4,6 +4,7 @@
 // result hand-off of ProcessProblem (main.cpp:599-626).
 #include "ctx.hpp"
 #include "pm_kernels.cuh"
+#include "aux_kernels.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -267,6 +268,36 @@ int Ctx::sample_view(int view, int n, const float* xy, float* out) {
     e = cudaMemcpyAsync(out, d_out, (size_t)n * 4, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cuda_fail(e, "download samples");
+    return HPM_OK;
+}
+
+// RunJBU (HPM.cpp:1266-1319): the coarser depths_geom map of a view upsampled to
+// the view's current image size into its depths map; nothing happens when the
+// integer scale is 1 (HPM.cpp:1272-1275).
+int Ctx::jbu_view(int view, int* applied) {
+    cudaSetDevice(device);
+    if (applied) *applied = 0;
+    if (view < 0 || view >= HPM_MAX_VIEWS || views[view].w == 0) return fail(HPM_E_STATE, "view %d not set", view);
+    ViewState& v = views[view];
+    const DevMap& src = v.maps[HPM_MAP_DEPTH_GEOM];
+    if (!src.ptr || src.w <= 0) return fail(HPM_E_STATE, "view %d has no depths_geom map", view);
+    const int scale = std::max(v.h / src.h, v.w / src.w);
+    if (scale == 1) return HPM_OK;
+    if (src.w * 1LL * src.h > (long long)v.w * v.h) return fail(HPM_E_STATE, "JBU source larger than the image");
+    // the source map must survive while the output is written: stage it in scratch
+    const size_t ns = (size_t)src.w * src.h;
+    cudaError_t e = ensure_buf(scratch, scratch_cap, ns * 4 + 256);
+    if (e != cudaSuccess) return cuda_fail(e, "alloc scratch");
+    float* d_src = reinterpret_cast<float*>(scratch);
+    const int sw = src.w, sh = src.h;
+    e = cudaMemcpyAsync(d_src, src.ptr, ns * 4, cudaMemcpyDeviceToDevice, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "stage JBU source");
+    e = ensure_map(view, HPM_MAP_DEPTH, v.w, v.h);
+    if (e != cudaSuccess) return cuda_fail(e, "alloc depth map");
+    e = launch_jbu(v.gray, v.w, v.h, d_src, sw, sh, v.maps[HPM_MAP_DEPTH].ptr, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "JBU launch");
+    ++launches;
+    if (applied) *applied = 1;
     return HPM_OK;
 }
 

@@ -95,6 +95,39 @@ int hpm_run_patchmatch(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, co
 int hpm_eval_costs(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, const hpm_params *params, int n,
                    const int32_t *px, const float *planes, float *out);
 
+/* Colour image (BGR, 8 bits) of a view at the size of its maps, for the point
+ * colours of fusion (the rescaled image of RunFusion, main.cpp:863-865). */
+int hpm_set_color(hpm_ctx *ctx, int view, const uint8_t *bgr, int w, int h);
+
+/* RunJBU (HPM.cpp:1266-1319) + JointBilateralUpsampling (main.cpp:636-657):
+ * the view's coarser DEPTH_GEOM map upsampled, guided by the view's grey image,
+ * into its DEPTH map at the image size.  *applied = 0 and nothing is written
+ * when the integer scale is 1 (HPM.cpp:1272-1275). */
+int hpm_jbu(hpm_ctx *ctx, int view, int *applied);
+
+/* JBU_cu / JBU_cu_prior (HPM.cu:3037-3197) on host buffers: src_depth (sw x sh)
+ * and, when src_normal (3 floats/px) is given, normals, upsampled to the view's
+ * image size guided by its grey image.  Without normals the NaN fallback of
+ * RunJBU (HPM.cpp:1297-1300) applies. */
+int hpm_jbu_maps(hpm_ctx *ctx, int view, const float *src_depth, const float *src_normal, int sw, int sh,
+                 float *out_depth, float *out_normal);
+
+/* ConfidenceEvaluation (main.cpp:959-1109) over views 0..n_views-1 (view id ==
+ * index, as the reference assumes): reads each view's depth map of
+ * `depth_kind` (DEPTH or DEPTH_GEOM) and NORMAL, with the view's camera scaled
+ * to the map size; writes each view's CONF map.  Source lists are
+ * src_ids[src_off[i] .. src_off[i+1]).  *iterations receives the largest
+ * number of fixed-point iterations a view needed. */
+int hpm_confidence_eval(hpm_ctx *ctx, int n_views, const int32_t *src_off, const int32_t *src_ids, int depth_kind,
+                        int *iterations);
+
+/* RunFusion (main.cpp:823-957), or RunFusion_Sky_Strict (main.cpp:659-821) when
+ * sky_masks (per view, BGR at the map size) is given.  Points in the
+ * reference's order; up to `capacity` are copied to `out`, the total count goes
+ * to *n_points.  Colours come from hpm_set_color. */
+int hpm_fuse(hpm_ctx *ctx, int n_views, const int32_t *src_off, const int32_t *src_ids, int depth_kind,
+             const uint8_t *const *sky_masks, hpm_point *out, int64_t capacity, int64_t *n_points);
+
 /* Diagnostic: n linear-filtered fetches of view `view`'s image through the
  * texture unit at unnormalised coordinates xy[2k], xy[2k+1] (tex2D as used by
  * HPM.cu:409).  No reference counterpart: pins the filter model of the tests. */

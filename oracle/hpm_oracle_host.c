@@ -50,8 +50,10 @@ static void project_cam(f3 X, const hpm_camera *c, f2 *pt, float *depth) /* HPM.
 
 static float angle_between(const float *a, const float *b) /* HPM.cpp:281-290 */
 {
+    /* acosf evaluated as the double acos rounded once (include/hpm_fp.h), so CPU
+     * and GPU agree bit for bit; it differs from a libm acosf by at most 1 ulp */
     const float dot = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
-    const float ang = acosf(dot);
+    const float ang = (float)acos((double)dot);
     if (ang != ang) return 0.0f;
     return ang;
 }
