@@ -40,7 +40,8 @@ EXPORTED_SYMBOLS = (
     "hpm_create", "hpm_destroy", "hpm_last_error", "hpm_set_view", "hpm_set_map", "hpm_get_map",
     "hpm_set_canny", "hpm_set_prior", "hpm_run_patchmatch", "hpm_eval_costs", "hpm_set_address_mode",
     "hpm_launch_count", "hpm_synchronize", "hpm_sample_view", "hpm_debug_run_partial", "hpm_set_color",
-    "hpm_jbu", "hpm_jbu_maps", "hpm_confidence_eval", "hpm_fuse",
+    "hpm_jbu", "hpm_jbu_maps", "hpm_confidence_eval", "hpm_fuse", "hpm_support_points", "hpm_delaunay",
+    "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior",
 )
 
 
@@ -168,6 +169,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.hpm_synchronize.argtypes = [vp]
     lib.hpm_sample_view.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp]
     lib.hpm_set_color.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int]
+    ip = ctypes.POINTER(ctypes.c_int)
+    lib.hpm_support_points.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ip, ip, ip]
+    lib.hpm_delaunay.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ip]
+    lib.hpm_prior_from_triangles.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int]
+    lib.hpm_build_prior.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip]
+    lib.hpm_get_prior.argtypes = [vp, ctypes.c_int, vp, vp]
     lib.hpm_jbu.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.hpm_jbu_maps.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
     lib.hpm_confidence_eval.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -184,6 +191,19 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 def _ptr(a: np.ndarray) -> ctypes.c_void_p:
     return ctypes.c_void_p(a.ctypes.data)
+
+
+def delaunay(xy: np.ndarray, width: int, height: int) -> np.ndarray:
+    """hpm_delaunay: triangles (n, 6) int32 of integer points in [0,w)x[0,h) (host only)."""
+    lib = load_library()
+    p = np.ascontiguousarray(xy, np.int32).reshape(-1, 2)
+    n = ctypes.c_int()
+    cap = 2 * p.shape[0] + 8
+    out = np.zeros((cap, 6), np.int32)
+    rc = lib.hpm_delaunay(_ptr(p) if p.size else None, p.shape[0], width, height, _ptr(out), cap, ctypes.byref(n))
+    if rc != 0:
+        raise HPMError(f"hpm_delaunay failed ({rc})")
+    return out[: n.value].copy()
 
 
 class Context:
@@ -342,6 +362,33 @@ class Context:
         self._check(self.lib.hpm_fuse(self.h, len(src_lists), _ptr(off), _ptr(ids), depth_kind, sky_arr, _ptr(out),
                                       capacity, ctypes.byref(n)), "hpm_fuse")
         return out[: min(n.value, capacity)], n.value
+
+    def support_points(self, view: int, distance: int = 0):
+        n, w, h = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.hpm_support_points(self.h, view, distance, None, 0, ctypes.byref(n), ctypes.byref(w),
+                                                ctypes.byref(h)), "hpm_support_points")
+        out = np.zeros((max(n.value, 1), 2), np.int32)
+        self._check(self.lib.hpm_support_points(self.h, view, distance, _ptr(out), n.value, None, None, None),
+                    "hpm_support_points")
+        return out[: n.value], (w.value, h.value)
+
+    def prior_from_triangles(self, view: int, distance: int, tris: np.ndarray) -> None:
+        t = np.ascontiguousarray(tris, np.int32).reshape(-1, 6)
+        self._check(self.lib.hpm_prior_from_triangles(self.h, view, distance, _ptr(t) if t.size else None,
+                                                      t.shape[0]), "hpm_prior_from_triangles")
+
+    def build_prior(self, view: int, distance: int = 0):
+        n_p, n_t = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.hpm_build_prior(self.h, view, distance, ctypes.byref(n_p), ctypes.byref(n_t)),
+                    "hpm_build_prior")
+        return n_p.value, n_t.value
+
+    def get_prior(self, view: int):
+        w, h = self.views[view]
+        planes = np.empty((h, w, 4), np.float32)
+        mask = np.empty((h, w), np.uint8)
+        self._check(self.lib.hpm_get_prior(self.h, view, _ptr(planes), _ptr(mask)), "hpm_get_prior")
+        return planes, mask
 
     def synchronize(self) -> None:
         self._check(self.lib.hpm_synchronize(self.h), "hpm_synchronize")

@@ -5,6 +5,12 @@
 #include "ctx.hpp"
 #include "pm_kernels.cuh"
 #include "aux_kernels.cuh"
+#include <cmath>
+#include <vector>
+
+namespace hpm {
+int delaunay_triangulate(const int32_t* xy, int n, int width, int height, std::vector<hpm_triangle>& out);
+}
 
 #include <algorithm>
 #include <cstdarg>
@@ -73,7 +79,9 @@ Ctx::~Ctx() {
         if (v.color) cudaFree(v.color);
     }
     for (void* p : { (void*)planes, (void*)costs, (void*)pre_costs, (void*)sel, (void*)rng, (void*)conf,
-                     (void*)scaled, (void*)scratch, (void*)scan_state, (void*)scan_work, (void*)points })
+                     (void*)scaled, (void*)scratch, (void*)scan_state, (void*)scan_work, (void*)points,
+                     (void*)prior_small, (void*)prior_tris, (void*)prior_label, (void*)prior_work,
+                     (void*)prior_unormal })
         if (p) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -359,6 +367,66 @@ int hpm_fuse(hpm_ctx* ctx, int n_views, const int32_t* src_off, const int32_t* s
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
         if (e != cudaSuccess) return c->cuda_fail(e, "download points");
     }
+    return HPM_OK;
+}
+
+int hpm_support_points(hpm_ctx* ctx, int view, int distance, int32_t* xy, int capacity, int* n, int* w, int* h) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || c->views[view].w == 0) return c->fail(HPM_E_STATE, "view %d not set", view);
+    if (distance < 0 || distance > 2) return c->fail(HPM_E_INVALID, "prior scale distance must be 0, 1 or 2");
+    std::vector<int32_t> pts;
+    int sw = 0, sh = 0;
+    int rc = c->support_points(view, distance, pts, sw, sh);
+    if (rc) return rc;
+    const int np = (int)pts.size() / 2;
+    if (n) *n = np;
+    if (w) *w = sw;
+    if (h) *h = sh;
+    if (xy) std::copy(pts.begin(), pts.begin() + 2 * std::min(np, std::max(capacity, 0)), xy);
+    return HPM_OK;
+}
+
+int hpm_delaunay(const int32_t* xy, int n, int w, int h, hpm_triangle* out, int capacity, int* n_out) {
+    if (n < 0 || (n > 0 && !xy) || w <= 0 || h <= 0) return HPM_E_INVALID;
+    std::vector<hpm_triangle> tris;
+    delaunay_triangulate(xy, n, w, h, tris);
+    if (n_out) *n_out = (int)tris.size();
+    if (out) std::copy(tris.begin(), tris.begin() + std::min((int)tris.size(), std::max(capacity, 0)), out);
+    return HPM_OK;
+}
+
+int hpm_prior_from_triangles(hpm_ctx* ctx, int view, int distance, const hpm_triangle* tris, int n_tris) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || c->views[view].w == 0) return c->fail(HPM_E_STATE, "view %d not set", view);
+    if (distance < 0 || distance > 2 || n_tris < 0 || (n_tris > 0 && !tris))
+        return c->fail(HPM_E_INVALID, "hpm_prior_from_triangles: bad arguments");
+    int sw = c->views[view].w, sh = c->views[view].h;
+    if (distance > 0) {
+        const float f = 1.0f / (distance * 2);
+        sw = (int)std::round(sw * f);
+        sh = (int)std::round(sh * f);
+    }
+    return c->prior_from_triangles(view, distance, tris, n_tris, sw, sh);
+}
+
+int hpm_build_prior(hpm_ctx* ctx, int view, int distance, int* n_points, int* n_triangles) {
+    if (!ctx) return HPM_E_INVALID;
+    return reinterpret_cast<Ctx*>(ctx)->build_prior(view, distance, n_points, n_triangles);
+}
+
+int hpm_get_prior(hpm_ctx* ctx, int view, float* planes, uint8_t* mask) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || !c->views[view].prior) return c->fail(HPM_E_STATE, "view %d has no prior", view);
+    const ViewState& v = c->views[view];
+    const size_t n = (size_t)v.prior_w * v.prior_h;
+    cudaError_t e = cudaSuccess;
+    if (planes) e = cudaMemcpyAsync(planes, v.prior, 16 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && mask) e = cudaMemcpyAsync(mask, v.pmask, n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "download prior");
     return HPM_OK;
 }
 

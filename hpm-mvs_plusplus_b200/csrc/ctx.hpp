@@ -63,6 +63,11 @@ struct Ctx {
     uint8_t* scan_state = nullptr; size_t scan_state_cap = 0;
     uint8_t* scan_work = nullptr; size_t scan_work_cap = 0;
     hpm_point* points = nullptr; size_t points_cap = 0;
+    float* prior_small = nullptr; size_t prior_small_cap = 0;
+    uint8_t* prior_tris = nullptr; size_t prior_tris_cap = 0;
+    int* prior_label = nullptr; size_t prior_label_cap = 0;
+    float* prior_work = nullptr; size_t prior_work_cap = 0;
+    float* prior_unormal = nullptr; size_t prior_unormal_cap = 0;
 
     ~Ctx();
     int fail(int code, const char* fmt, ...);
@@ -84,6 +89,10 @@ struct Ctx {
                          const uint8_t* const* sky_host, hpm_point* out_device, int64_t capacity, int64_t* n_points,
                          int* max_iterations_used);
     int jbu_view(int view, int* applied);
+    int prior_downsample(int view, int distance, int& hw, int& hh);
+    int support_points(int view, int distance, std::vector<int32_t>& xy, int& sup_w, int& sup_h);
+    int prior_from_triangles(int view, int distance, const hpm_triangle* tris, int n_tris, int sup_w, int sup_h);
+    int build_prior(int view, int distance, int* n_points, int* n_triangles);
     int eval_costs(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n, const int32_t* px,
                    const float* planes, float* out);
 };

@@ -128,6 +128,30 @@ int hpm_confidence_eval(hpm_ctx *ctx, int n_views, const int32_t *src_off, const
 int hpm_fuse(hpm_ctx *ctx, int n_views, const int32_t *src_off, const int32_t *src_ids, int depth_kind,
              const uint8_t *const *sky_masks, hpm_point *out, int64_t capacity, int64_t *n_points);
 
+/* Support points of the planar prior (GetSupportPoints_Classify_Check,
+ * HPM.cpp:1026-1073) from the view's COST and CONF maps; with distance 1 or 2
+ * the maps are first downsampled by 1/(2*distance) (main.cpp:444-454).  Up to
+ * `capacity` (x, y) pairs are written, *n gets the count, *w x *h the size of
+ * the rectangle they live in. */
+int hpm_support_points(hpm_ctx *ctx, int view, int distance, int32_t *xy, int capacity, int *n, int *w, int *h);
+
+/* Delaunay triangulation of integer points inside [0,w)x[0,h) (the role of
+ * cv::Subdiv2D in HPM::DelaunayTriangulation, HPM.cpp:1075-1097).  Host only;
+ * duplicate points are ignored. */
+int hpm_delaunay(const int32_t *xy, int n, int w, int h, hpm_triangle *out, int capacity, int *n_out);
+
+/* Planar prior of a view from a triangle list: raster (main.cpp:389-409),
+ * 3-point plane fits in double (HPM.cpp:1099-1167), prior depth mask and, for
+ * distance 1 or 2, prior JBU and reload (main.cpp:443-576).  The result is the
+ * prior hpm_run_patchmatch uses in prior mode. */
+int hpm_prior_from_triangles(hpm_ctx *ctx, int view, int distance, const hpm_triangle *tris, int n_tris);
+
+/* Support points -> Delaunay -> hpm_prior_from_triangles in one call. */
+int hpm_build_prior(hpm_ctx *ctx, int view, int distance, int *n_points, int *n_triangles);
+
+/* Download a view's prior: planes (4 floats per pixel) and mask (0/1). */
+int hpm_get_prior(hpm_ctx *ctx, int view, float *planes, uint8_t *mask);
+
 /* Diagnostic: n linear-filtered fetches of view `view`'s image through the
  * texture unit at unnormalised coordinates xy[2k], xy[2k+1] (tex2D as used by
  * HPM.cu:409).  No reference counterpart: pins the filter model of the tests. */

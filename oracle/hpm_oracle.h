@@ -152,6 +152,10 @@ int32_t ora_planar_prior(const hpm_triangle *tris, int32_t n_tris, const float *
                          float *mask_out, float *planes_out, float *prior_depth_out,
                          float *prior_normal_out);
 
+/* Reload of an upsampled prior (main.cpp:548-570): camera-frame planes and mask. */
+void ora_prior_reload(const float *udepth, const float *unormal, int W, int H, const hpm_camera *c, float dmin,
+                      float dmax, float *prior, uint8_t *mask);
+
 /* Philox4x32-10 block and uniform draw of include/hpm_philox.h. */
 void ora_philox(const uint32_t ctr[4], uint32_t k0, uint32_t k1, uint32_t out[4]);
 float ora_uniform(uint64_t seed, uint32_t view, uint32_t x, uint32_t y, uint32_t draw);

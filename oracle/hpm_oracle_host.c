@@ -319,17 +319,19 @@ int32_t ora_planar_prior(const hpm_triangle *tris, int32_t n_tris, const float *
     return (int32_t)idx;
 }
 
-/* cv::resize(..., INTER_LINEAR) for one float channel: half-pixel centres,
- * taps clamped at the borders. */
+/* cv::resize(..., INTER_LINEAR) for one float channel: half-pixel centres, taps
+ * clamped at the borders.  The source coordinate is formed in double, and each
+ * pass output is the two-tap sum evaluated exactly and rounded once; this agrees
+ * with OpenCV 4.x to within 1 ulp (its SIMD kernels round differently). */
 void ora_resize_linear_f32(const float *src, int sw, int sh, float *dst, int dw, int dh)
 {
     const double sx_scale = 1.0 / ((double)dw / sw), sy_scale = 1.0 / ((double)dh / sh);
     int *xo = (int *)malloc(sizeof(int) * 2 * (size_t)dw);
     float *xa = (float *)malloc(sizeof(float) * 2 * (size_t)dw);
     for (int dx = 0; dx < dw; ++dx) {
-        float fx = (float)((dx + 0.5) * sx_scale - 0.5);
-        int sx = (int)floorf(fx);
-        fx -= sx;
+        const double fxd = (dx + 0.5) * sx_scale - 0.5;
+        int sx = (int)floor(fxd);
+        float fx = (float)(fxd - sx);
         if (sx < 0) { fx = 0; sx = 0; }
         if (sx >= sw - 1) { fx = 0; sx = sw - 1; }
         xo[2 * dx] = sx; xo[2 * dx + 1] = sx + 1 < sw ? sx + 1 : sw - 1;
@@ -338,18 +340,43 @@ void ora_resize_linear_f32(const float *src, int sw, int sh, float *dst, int dw,
     float *r0 = (float *)malloc(sizeof(float) * (size_t)dw);
     float *r1 = (float *)malloc(sizeof(float) * (size_t)dw);
     for (int dy = 0; dy < dh; ++dy) {
-        float fy = (float)((dy + 0.5) * sy_scale - 0.5);
-        int sy = (int)floorf(fy);
-        fy -= sy;
+        const double fyd = (dy + 0.5) * sy_scale - 0.5;
+        int sy = (int)floor(fyd);
+        float fy = (float)(fyd - sy);
         if (sy < 0) { fy = 0; sy = 0; }
         if (sy >= sh - 1) { fy = 0; sy = sh - 1; }
         const int sy1 = sy + 1 < sh ? sy + 1 : sh - 1;
         for (int dx = 0; dx < dw; ++dx) {
-            r0[dx] = src[sy * sw + xo[2 * dx]] * xa[2 * dx] + src[sy * sw + xo[2 * dx + 1]] * xa[2 * dx + 1];
-            r1[dx] = src[sy1 * sw + xo[2 * dx]] * xa[2 * dx] + src[sy1 * sw + xo[2 * dx + 1]] * xa[2 * dx + 1];
+            r0[dx] = (float)((double)src[sy * sw + xo[2 * dx]] * xa[2 * dx] + (double)src[sy * sw + xo[2 * dx + 1]] * xa[2 * dx + 1]);
+            r1[dx] = (float)((double)src[sy1 * sw + xo[2 * dx]] * xa[2 * dx] + (double)src[sy1 * sw + xo[2 * dx + 1]] * xa[2 * dx + 1]);
         }
         const float b0 = 1.0f - fy, b1 = fy;
-        for (int dx = 0; dx < dw; ++dx) dst[dy * dw + dx] = r0[dx] * b0 + r1[dx] * b1;
+        for (int dx = 0; dx < dw; ++dx) dst[dy * dw + dx] = (float)((double)r0[dx] * b0 + (double)r1[dx] * b1);
     }
     free(xo); free(xa); free(r0); free(r1);
+}
+
+void ora_prior_reload(const float *udepth, const float *unormal, int W, int H, const hpm_camera *c, float dmin,
+                      float dmax, float *prior, uint8_t *mask)
+{
+    /* main.cpp:548-570 with TransformNormal2RefCam (HPM.cpp:1189-1197) and
+     * GetDistance2Origin (HPM.cpp:1199-1206) */
+    for (int j = 0; j < H; ++j)
+        for (int i = 0; i < W; ++i) {
+            const size_t k = (size_t)j * W + i;
+            const float d = udepth[k];
+            float *pl = prior + 4 * k;
+            pl[0] = pl[1] = pl[2] = pl[3] = 0.0f;
+            mask[k] = 0;
+            if (d <= dmax && d >= dmin) {
+                const float a = unormal[3 * k], b = unormal[3 * k + 1], e = unormal[3 * k + 2];
+                pl[0] = c->R[0] * a + c->R[1] * b + c->R[2] * e;
+                pl[1] = c->R[3] * a + c->R[4] * b + c->R[5] * e;
+                pl[2] = c->R[6] * a + c->R[7] * b + c->R[8] * e;
+                const float X0 = d * (i - c->K[2]) / (c->K[0]);
+                const float X1 = d * (j - c->K[5]) / (c->K[4]);
+                pl[3] = -(pl[0] * X0 + pl[1] * X1 + pl[2] * d);
+                mask[k] = 1;
+            }
+        }
 }

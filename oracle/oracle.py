@@ -95,6 +95,8 @@ def lib() -> ctypes.CDLL:
                                        ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, vp, vp, vp, vp]
         L.ora_resize_linear_f32.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int]
         L.ora_philox.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
+        L.ora_prior_reload.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Camera), ctypes.c_float,
+                                       ctypes.c_float, vp, vp]
         L.ora_uniform.restype = ctypes.c_float
         L.ora_uniform.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
     return _lib
@@ -303,3 +305,14 @@ def resize_linear(src: np.ndarray, dw: int, dh: int) -> np.ndarray:
     out = np.empty((dh, dw), np.float32)
     lib().ora_resize_linear_f32(_p(src), src.shape[1], src.shape[0], _p(out), dw, dh)
     return out
+
+
+def prior_reload(udepth: np.ndarray, unormal: np.ndarray, cam, dmin: float, dmax: float):
+    udepth = np.ascontiguousarray(udepth, np.float32)
+    unormal = np.ascontiguousarray(unormal, np.float32)
+    H, W = udepth.shape
+    prior = np.zeros((H, W, 4), np.float32)
+    mask = np.zeros((H, W), np.uint8)
+    c = to_cam(cam)
+    lib().ora_prior_reload(_p(udepth), _p(unormal), W, H, ctypes.byref(c), dmin, dmax, _p(prior), _p(mask))
+    return prior, mask
