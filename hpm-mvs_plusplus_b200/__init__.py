@@ -41,8 +41,16 @@ EXPORTED_SYMBOLS = (
     "hpm_set_canny", "hpm_set_prior", "hpm_run_patchmatch", "hpm_eval_costs", "hpm_set_address_mode",
     "hpm_launch_count", "hpm_synchronize", "hpm_sample_view", "hpm_debug_run_partial", "hpm_set_color",
     "hpm_jbu", "hpm_jbu_maps", "hpm_confidence_eval", "hpm_fuse", "hpm_support_points", "hpm_delaunay",
-    "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior",
+    "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior", "hpm_set_image", "hpm_prepare_level",
+    "hpm_get_level", "hpm_reconstruct", "hpm_get_points",
 )
+
+
+class ReconOptions(ctypes.Structure):
+    """hpm_recon_options: --initial-image-scale, geometric iterations, fusion, seed."""
+
+    _fields_ = [("initial_image_scale", ctypes.c_int32), ("geom_iterations", ctypes.c_int32),
+                ("fuse", ctypes.c_int32), ("level_max_side", ctypes.c_int32), ("seed", ctypes.c_uint64)]
 
 
 class Point(ctypes.Structure):
@@ -175,6 +183,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.hpm_prior_from_triangles.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int]
     lib.hpm_build_prior.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip, ip]
     lib.hpm_get_prior.argtypes = [vp, ctypes.c_int, vp, vp]
+    lib.hpm_set_image.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int]
+    lib.hpm_prepare_level.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Camera)]
+    lib.hpm_get_level.argtypes = [vp, ctypes.c_int, vp, vp, vp]
+    lib.hpm_reconstruct.argtypes = [vp, ctypes.c_int, vp, vp, vp, ctypes.POINTER(ReconOptions),
+                                    ctypes.POINTER(ctypes.c_int64)]
+    lib.hpm_get_points.argtypes = [vp, vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     lib.hpm_jbu.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.hpm_jbu_maps.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
     lib.hpm_confidence_eval.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -389,6 +403,41 @@ class Context:
         mask = np.empty((h, w), np.uint8)
         self._check(self.lib.hpm_get_prior(self.h, view, _ptr(planes), _ptr(mask)), "hpm_get_prior")
         return planes, mask
+
+    def set_image(self, view: int, bgr: np.ndarray) -> None:
+        c = np.ascontiguousarray(bgr, dtype=np.uint8)
+        h, w = c.shape[:2]
+        self._check(self.lib.hpm_set_image(self.h, view, _ptr(c), w, h), "hpm_set_image")
+
+    def prepare_level(self, view: int, w: int, h: int, cam: Camera) -> None:
+        self._check(self.lib.hpm_prepare_level(self.h, view, w, h, ctypes.byref(cam)), "hpm_prepare_level")
+        self.views[view] = (w, h)
+
+    def get_level(self, view: int):
+        w, h = self.views[view]
+        bgr = np.empty((h, w, 3), np.uint8)
+        gray = np.empty((h, w), np.float32)
+        edges = np.empty((h, w), np.uint8)
+        self._check(self.lib.hpm_get_level(self.h, view, _ptr(bgr), _ptr(gray), _ptr(edges)), "hpm_get_level")
+        return bgr, gray, edges
+
+    def reconstruct(self, cams, src_lists, initial_image_scale: int = 4, seed: int = 0, fuse: bool = True,
+                    geom_iterations: int = 3, level_max_side: int = 0) -> int:
+        cam_arr = (Camera * len(cams))(*cams)
+        off, ids = self._src_lists(src_lists)
+        opt = ReconOptions(initial_image_scale, geom_iterations, 1 if fuse else 0, level_max_side, seed)
+        n = ctypes.c_int64()
+        self._check(self.lib.hpm_reconstruct(self.h, len(cams), cam_arr, _ptr(off), _ptr(ids), ctypes.byref(opt),
+                                             ctypes.byref(n)), "hpm_reconstruct")
+        return n.value
+
+    def get_points(self, capacity: int | None = None) -> np.ndarray:
+        n = ctypes.c_int64()
+        self._check(self.lib.hpm_get_points(self.h, None, 0, ctypes.byref(n)), "hpm_get_points")
+        cap = n.value if capacity is None else min(capacity, n.value)
+        out = np.zeros((max(cap, 1), 9), np.float32)
+        self._check(self.lib.hpm_get_points(self.h, _ptr(out), cap, None), "hpm_get_points")
+        return out[:cap]
 
     def synchronize(self) -> None:
         self._check(self.lib.hpm_synchronize(self.h), "hpm_synchronize")

@@ -77,11 +77,12 @@ Ctx::~Ctx() {
         if (v.prior) cudaFree(v.prior);
         if (v.pmask) cudaFree(v.pmask);
         if (v.color) cudaFree(v.color);
+        if (v.orig) cudaFree(v.orig);
     }
     for (void* p : { (void*)planes, (void*)costs, (void*)pre_costs, (void*)sel, (void*)rng, (void*)conf,
                      (void*)scaled, (void*)scratch, (void*)scan_state, (void*)scan_work, (void*)points,
                      (void*)prior_small, (void*)prior_tris, (void*)prior_label, (void*)prior_work,
-                     (void*)prior_unormal })
+                     (void*)prior_unormal, (void*)canny_mag, (void*)canny_grad, (void*)canny_state })
         if (p) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -360,6 +361,7 @@ int hpm_fuse(hpm_ctx* ctx, int n_views, const int32_t* src_off, const int32_t* s
     int rc = c->consistency_scan(1, n_views, src_off, src_ids, depth_kind, sky_masks, c->points, (int64_t)total, &n,
                                  nullptr);
     if (rc) return rc;
+    c->n_points = n;
     if (n_points) *n_points = n;
     if (out && capacity > 0) {
         const int64_t m = n < capacity ? n : capacity;
@@ -427,6 +429,62 @@ int hpm_get_prior(hpm_ctx* ctx, int view, float* planes, uint8_t* mask) {
     if (e == cudaSuccess && mask) e = cudaMemcpyAsync(mask, v.pmask, n, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return c->cuda_fail(e, "download prior");
+    return HPM_OK;
+}
+
+int hpm_set_image(hpm_ctx* ctx, int view, const uint8_t* bgr, int w, int h) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || !bgr || w <= 0 || h <= 0)
+        return c->fail(HPM_E_INVALID, "hpm_set_image: bad arguments");
+    cudaSetDevice(c->device);
+    ViewState& v = c->views[view];
+    cudaError_t e = ensure(v.orig, v.orig_cap, (size_t)w * h * 3);
+    if (e != cudaSuccess) return c->cuda_fail(e, "alloc image");
+    e = cudaMemcpyAsync(v.orig, bgr, (size_t)w * h * 3, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "upload image");
+    v.orig_w = w; v.orig_h = h;
+    return HPM_OK;
+}
+
+int hpm_prepare_level(hpm_ctx* ctx, int view, int w, int h, const hpm_camera* cam) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || !cam || w <= 0 || h <= 0)
+        return c->fail(HPM_E_INVALID, "hpm_prepare_level: bad arguments");
+    return c->prepare_level_image(view, w, h, *cam);
+}
+
+int hpm_get_level(hpm_ctx* ctx, int view, uint8_t* bgr, float* gray, uint8_t* edges) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (view < 0 || view >= HPM_MAX_VIEWS || c->views[view].w == 0) return c->fail(HPM_E_STATE, "view %d not set", view);
+    const ViewState& v = c->views[view];
+    const size_t n = (size_t)v.w * v.h;
+    cudaError_t e = cudaSuccess;
+    if (bgr && v.color) e = cudaMemcpyAsync(bgr, v.color, n * 3, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && gray) e = cudaMemcpyAsync(gray, v.gray, n * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && edges && v.canny) e = cudaMemcpyAsync(edges, v.canny, n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "download level image");
+    return HPM_OK;
+}
+
+int hpm_reconstruct(hpm_ctx* ctx, int n_views, const hpm_camera* cams, const int32_t* src_off, const int32_t* src_ids,
+                    const hpm_recon_options* opt, int64_t* n_points) {
+    if (!ctx) return HPM_E_INVALID;
+    return reinterpret_cast<Ctx*>(ctx)->reconstruct(n_views, cams, src_off, src_ids, opt, n_points);
+}
+
+int hpm_get_points(hpm_ctx* ctx, hpm_point* out, int64_t capacity, int64_t* n_points) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (n_points) *n_points = c->n_points;
+    if (!out || capacity <= 0 || c->n_points == 0) return HPM_OK;
+    const int64_t m = c->n_points < capacity ? c->n_points : capacity;
+    cudaError_t e = cudaMemcpyAsync(out, c->points, sizeof(hpm_point) * (size_t)m, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return c->cuda_fail(e, "download points");
     return HPM_OK;
 }
 

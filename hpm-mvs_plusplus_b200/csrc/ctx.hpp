@@ -36,6 +36,9 @@ struct ViewState {
     uint8_t* pmask = nullptr;
     size_t pmask_cap = 0;
     int prior_w = 0, prior_h = 0;
+    uint8_t* orig = nullptr;   // original BGR image (images/%08d.jpg)
+    size_t orig_cap = 0;
+    int orig_w = 0, orig_h = 0;
     uint8_t* color = nullptr;  // BGR at the map size (fusion colours)
     size_t color_cap = 0;
     int color_w = 0, color_h = 0;
@@ -68,6 +71,10 @@ struct Ctx {
     int* prior_label = nullptr; size_t prior_label_cap = 0;
     float* prior_work = nullptr; size_t prior_work_cap = 0;
     float* prior_unormal = nullptr; size_t prior_unormal_cap = 0;
+    int* canny_mag = nullptr; size_t canny_mag_cap = 0;
+    short2* canny_grad = nullptr; size_t canny_grad_cap = 0;
+    uint8_t* canny_state = nullptr; size_t canny_state_cap = 0;
+    int64_t n_points = 0;
 
     ~Ctx();
     int fail(int code, const char* fmt, ...);
@@ -93,6 +100,10 @@ struct Ctx {
     int support_points(int view, int distance, std::vector<int32_t>& xy, int& sup_w, int& sup_h);
     int prior_from_triangles(int view, int distance, const hpm_triangle* tris, int n_tris, int sup_w, int sup_h);
     int build_prior(int view, int distance, int* n_points, int* n_triangles);
+    int prepare_level_image(int view, int w, int h, const hpm_camera& cam);
+    int canny_view(int view);
+    int reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off, const int32_t* src_ids,
+                    const hpm_recon_options* opt, int64_t* n_points_out);
     int eval_costs(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n, const int32_t* px,
                    const float* planes, float* out);
 };

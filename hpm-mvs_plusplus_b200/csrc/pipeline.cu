@@ -1,0 +1,183 @@
+// The reconstruction schedule of HPM-MVS++ main() (main.cpp:1183-1359) on
+// resident GPU data.  Where the reference hands every stage's result to the
+// next through .dmb files, the passes here read and write the per-view maps of
+// the context; the order of passes and of views inside a pass is the
+// reference's, so the geometric iterations that read neighbours' depths_geom
+// maps rewritten earlier in the same pass see the same (Gauss-Seidel) state.
+#include "ctx.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace hpm {
+
+namespace {
+
+uint64_t mix_seed(uint64_t base, uint64_t a, uint64_t b) {
+    uint64_t z = base ^ (a * 0x9E3779B97F4A7C15ULL) ^ (b * 0xBF58476D1CE4E5B9ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+}  // namespace
+
+int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off, const int32_t* src_ids,
+                     const hpm_recon_options* opt, int64_t* n_points_out) {
+    cudaSetDevice(device);
+    if (n_views < 1 || n_views > HPM_MAX_VIEWS || !cams || !src_off || !src_ids || !opt)
+        return fail(HPM_E_INVALID, "hpm_reconstruct: bad arguments");
+    if (opt->initial_image_scale < 1) return fail(HPM_E_INVALID, "--initial-image-scale must be at least 1");
+    for (int i = 0; i < n_views; ++i) {
+        if (!views[i].orig || views[i].orig_w <= 0) return fail(HPM_E_STATE, "view %d has no image", i);
+        const int ns = src_off[i + 1] - src_off[i];
+        if (ns < 1 || ns > HPM_MAX_SRC) return fail(HPM_E_INVALID, "view %d has %d sources (1..31)", i, ns);
+    }
+    const int scale = opt->initial_image_scale;
+    const int geom_iterations = opt->geom_iterations > 0 ? opt->geom_iterations : 3;
+    const int size_bound = opt->level_max_side > 0 ? opt->level_max_side : 1000;
+
+    // ComputeMultiScaleSettings (main.cpp:202-235)
+    std::vector<int> initial_max_side(n_views), num_downscale(n_views), cur_max_side(n_views, 0);
+    int max_num_downscale = -1;
+    for (int i = 0; i < n_views; ++i) {
+        const int original = std::max(views[i].orig_w, views[i].orig_h);
+        initial_max_side[i] = std::max(1, (original + scale / 2) / scale);
+        int k = 0, side = initial_max_side[i];
+        while (side > size_bound) { side /= 2; ++k; }
+        num_downscale[i] = k;
+        max_num_downscale = std::max(max_num_downscale, k);
+    }
+    const int max_hpm_scale = max_num_downscale;
+    std::vector<int> ids(n_views);
+    for (int i = 0; i < n_views; ++i) ids[i] = i;
+    int pass = 0;
+    int rc = HPM_OK;
+
+    auto run = [&](int i, uint32_t mode, int texture_level) -> int {
+        const hpm_camera& c = views[i].cam;
+        hpm_params p;
+        p.max_iterations = 3;  // RunPatchMatch hard-codes 3 (HPM.cu:3013)
+        p.patch_size = 11;
+        p.radius_increment = 2;
+        p.sigma_spatial = 5.0f;
+        p.sigma_color = 3.0f;
+        p.top_k = 4;
+        p.depth_min = c.depth_min * 0.6f;
+        p.depth_max = c.depth_max * 1.2f;
+        p.num_images = src_off[i + 1] - src_off[i] + 1;
+        p.scaled_cols = 0;
+        p.scaled_rows = 0;
+        p.mode = mode;
+        return run_patchmatch(i, src_ids + src_off[i], p.num_images - 1, &p, texture_level,
+                              mix_seed(opt->seed, (uint64_t)pass, (uint64_t)i));
+    };
+    auto confidence = [&](int depth_kind) -> int {
+        return consistency_scan(0, n_views, src_off, src_ids, depth_kind, nullptr, nullptr, 0, nullptr, nullptr);
+    };
+    auto prior_passes = [&](int level) -> int {
+        for (int hpm_scale = max_hpm_scale; hpm_scale >= level; --hpm_scale) {
+            int r = confidence(HPM_MAP_DEPTH);
+            if (r) return r;
+            ++pass;
+            for (int i = 0; i < n_views; ++i) {
+                const int distance = hpm_scale - num_downscale[i] - 1;
+                if (distance < 0 || distance > 2)
+                    return fail(HPM_E_STATE, "view %d: prior scale distance %d is outside 0..2", i, distance);
+                r = build_prior(i, distance, nullptr, nullptr);
+                if (r) return r;
+                r = run(i, HPM_MODE_PRIOR, level);
+                if (r) return r;
+            }
+        }
+        return HPM_OK;
+    };
+    auto geom_passes = [&](int level) -> int {
+        for (int it = 0; it < geom_iterations; ++it) {
+            uint32_t mode = HPM_MODE_GEOM;
+            if (it > 0) {
+                mode |= HPM_MODE_MULTIGEOM | HPM_MODE_MAND;
+                int r = confidence(HPM_MAP_DEPTH_GEOM);
+                if (r) return r;
+            }
+            ++pass;
+            for (int i = 0; i < n_views; ++i) {
+                int r = run(i, mode, level);
+                if (r) return r;
+            }
+        }
+        return HPM_OK;
+    };
+
+    bool first = true;
+    while (max_num_downscale >= 0) {
+        for (int i = 0; i < n_views; ++i) {
+            if (num_downscale[i] >= 0) {
+                cur_max_side[i] = (int)(initial_max_side[i] / std::pow(2.0, num_downscale[i]));
+                num_downscale[i]--;
+            }
+        }
+        // PrepareScaleImages (main.cpp:107-161) + InuputInitialization's camera scaling (HPM.cpp:668-676)
+        for (int i = 0; i < n_views; ++i) {
+            ViewState& v = views[i];
+            int w = v.orig_w, h = v.orig_h;
+            const int target = cur_max_side[i];
+            if (std::max(w, h) > target) {
+                const float factor = std::min((float)target / w, (float)target / h);
+                w = std::max(1, (int)std::round(v.orig_w * factor));
+                h = std::max(1, (int)std::round(v.orig_h * factor));
+            }
+            hpm_camera c = cams[i];
+            const float sx = w / (float)v.orig_w, sy = h / (float)v.orig_h;
+            c.K[0] *= sx; c.K[2] *= sx; c.K[4] *= sy; c.K[5] *= sy;
+            rc = prepare_level_image(i, w, h, c);
+            if (rc) return rc;
+        }
+        const int level = max_num_downscale;
+        if (first) {
+            first = false;
+            ++pass;
+            for (int i = 0; i < n_views; ++i)
+                if ((rc = run(i, 0, level))) return rc;
+            if ((rc = prior_passes(level))) return rc;
+            if ((rc = geom_passes(level))) return rc;
+        } else {
+            for (int i = 0; i < n_views; ++i) {
+                int applied = 0;
+                if ((rc = jbu_view(i, &applied))) return rc;
+            }
+            ++pass;
+            for (int i = 0; i < n_views; ++i)
+                if ((rc = run(i, HPM_MODE_HIERARCHY, level))) return rc;
+            if ((rc = prior_passes(level))) return rc;
+            if ((rc = geom_passes(level))) return rc;
+        }
+        --max_num_downscale;
+    }
+    n_points = 0;
+    if (opt->fuse) {
+        size_t total = 0;
+        for (int i = 0; i < n_views; ++i) total += (size_t)views[i].w * views[i].h;
+        cudaError_t e = cudaSuccess;
+        if (total + 1 > points_cap || !points) {
+            if (points) cudaFree(points);
+            points = nullptr;
+            points_cap = 0;
+            e = cudaMalloc((void**)&points, (total + 1) * sizeof(hpm_point));
+            if (e == cudaSuccess) points_cap = total + 1;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "alloc points");
+        int64_t n = 0;
+        rc = consistency_scan(1, n_views, src_off, src_ids, HPM_MAP_DEPTH_GEOM, nullptr, points, (int64_t)total, &n,
+                              nullptr);
+        if (rc) return rc;
+        n_points = n;
+    }
+    if (n_points_out) *n_points_out = n_points;
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "reconstruction");
+    return HPM_OK;
+}
+
+}  // namespace hpm

@@ -28,6 +28,16 @@ extern "C" {
 
 typedef struct hpm_ctx hpm_ctx;
 
+/* Options of a whole reconstruction (the command line of main.cpp:1143-1181). */
+typedef struct hpm_recon_options {
+    int32_t initial_image_scale; /* --initial-image-scale N (default 4) */
+    int32_t geom_iterations;     /* geometric iterations per level (3, main.cpp:1236) */
+    int32_t fuse;                /* run fusion after the last level */
+    int32_t level_max_side;      /* 0: 1000, the pyramid bound of ComputeMultiScaleSettings (main.cpp:205);
+                                    smaller values build more levels on small inputs */
+    uint64_t seed;               /* key of the random streams of all runs */
+} hpm_recon_options;
+
 enum {
     HPM_OK = 0,
     HPM_E_INVALID = 1,   /* bad argument */
@@ -151,6 +161,31 @@ int hpm_build_prior(hpm_ctx *ctx, int view, int distance, int *n_points, int *n_
 
 /* Download a view's prior: planes (4 floats per pixel) and mask (0/1). */
 int hpm_get_prior(hpm_ctx *ctx, int view, float *planes, uint8_t *mask);
+
+/* Original BGR image of a view (what images/%08d.jpg decodes to). */
+int hpm_set_image(hpm_ctx *ctx, int view, const uint8_t *bgr, int w, int h);
+
+/* Builds a view's pyramid-level image from its original: cv::resize INTER_LINEAR
+ * to w x h (PrepareScaleImages, main.cpp:107-161), BGR->grey as float
+ * (HPM.cpp:658-662), the level colour for fusion, and the Canny(50, 150) edge
+ * map (main.cpp:287).  `cam` is the camera scaled to w x h. */
+int hpm_prepare_level(hpm_ctx *ctx, int view, int w, int h, const hpm_camera *cam);
+
+/* Download a view's level image: BGR (w*h*3) and/or Canny edges (w*h). */
+int hpm_get_level(hpm_ctx *ctx, int view, uint8_t *bgr, float *gray, uint8_t *edges);
+
+/* The whole HPM-MVS++ schedule of main.cpp:1183-1359 on resident data: for
+ * views 0..n_views-1 with original images set by hpm_set_image and original
+ * cameras `cams` (as read from cams/%08d_cam.txt), source lists
+ * src_ids[src_off[i]..src_off[i+1]): pyramid levels, photometric, prior,
+ * hierarchy and geometric PatchMatch passes, JBU, confidence evaluations and
+ * (opt->fuse) fusion.  Final maps stay resident (DEPTH_GEOM, NORMAL, ...);
+ * points are read with hpm_get_points.  *n_points gets the fused count. */
+int hpm_reconstruct(hpm_ctx *ctx, int n_views, const hpm_camera *cams, const int32_t *src_off,
+                    const int32_t *src_ids, const hpm_recon_options *opt, int64_t *n_points);
+
+/* Copy up to `capacity` fused points of the last hpm_reconstruct / hpm_fuse. */
+int hpm_get_points(hpm_ctx *ctx, hpm_point *out, int64_t capacity, int64_t *n_points);
 
 /* Diagnostic: n linear-filtered fetches of view `view`'s image through the
  * texture unit at unnormalised coordinates xy[2k], xy[2k+1] (tex2D as used by

@@ -1,0 +1,64 @@
+"""REFERENCE BUILD wrapper -- test infrastructure only.
+
+ctypes binding of oracle/_ref/libhpmref.so: the reference's own CUDA kernels
+(HPM.cu of HPM-MVS++, compiled from its sources for sm_100a by
+oracle/ref_build.mk with its own --use_fast_math flags) driven through
+HPM::RunPatchMatch (HPM.cu:2987-3035).  Random draws are the shared Philox
+stream, so the reference build, the CPU oracle and the CUDA path start from the
+same hypotheses.  The library is built in the development container (the
+reference sources are read there) and travels prebuilt; where it is absent the
+callers skip.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+import hpm_oracle as ora
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libhpmref.so")
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        _lib.ref_run_patchmatch.restype = ctypes.c_int
+        _lib.ref_run_patchmatch.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ora.Params), vp, vp, vp, vp, vp,
+                                            vp, vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32,
+                                            ctypes.POINTER(ctypes.c_float)]
+    return _lib
+
+
+def _ptrs(arrs):
+    return (ctypes.c_void_p * len(arrs))(*[None if a is None else a.ctypes.data for a in arrs])
+
+
+def run_patchmatch(images, depths, cams, params, st: "ora.RunState", seed: int, view_id: int) -> float:
+    """Same arguments and state as hpm_oracle.run_patchmatch; returns the run's device time in ms."""
+    imgs = [np.ascontiguousarray(i, np.float32) for i in images]
+    deps = [np.zeros((1, 1), np.float32) if d is None else np.ascontiguousarray(d, np.float32)
+            for d in (depths or [None] * len(imgs))]
+    cam_arr = (ora.Camera * len(cams))(*[ora.to_cam(c) for c in cams])
+    prm = ora.to_params(params)
+    canny = np.ascontiguousarray(st.canny, np.uint32)
+    scaled = np.ascontiguousarray(st.scaled_planes, np.float32)
+    ms = ctypes.c_float(0.0)
+    rc = lib().ref_run_patchmatch(_ptrs(imgs), cam_arr, len(imgs), ctypes.byref(prm), st.planes.ctypes.data,
+                                  st.costs.ctypes.data, scaled.ctypes.data, st.prior_planes.ctypes.data,
+                                  st.plane_masks.ctypes.data, st.confidences.ctypes.data, canny.ctypes.data,
+                                  st.texture.ctypes.data, _ptrs(deps), ctypes.c_uint64(seed), view_id,
+                                  ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"reference build: CUDA error {rc}")
+    return float(ms.value)

@@ -1,0 +1,188 @@
+// CHECKER ONLY: drives the reference's own CUDA code (HPM.cu of HPM-MVS++,
+// compiled from its sources by oracle/ref_build.mk with the reference's flags)
+// on in-memory inputs.  It fills the members of an `HPM` object the way
+// HPM::CudaSpaceInitialization and friends do (HPM.cpp:741-984: one float
+// cudaArray per view with linear filtering and wrap addressing, per-pixel
+// buffers) and calls HPM::RunPatchMatch() (HPM.cu:2987-3035) unchanged.
+// Random draws come from oracle/ref_shim/ref_rng.h.  Used by
+// tests/test_ref_build.py and the reference-CUDA timing of bench.py.
+#define private public
+#include "HPM.h"
+#undef private
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+extern __device__ unsigned long long g_ref_seed;
+extern __device__ unsigned int g_ref_view;
+
+// HPM.cpp is not compiled (it needs OpenCV I/O); the three symbols of it that
+// HPM.cu links against are supplied here.
+void CudaSafeCall(const cudaError_t error, const std::string& file, const int line) {
+    if (error != cudaSuccess) fprintf(stderr, "reference CUDA error %s at %s:%d\n", cudaGetErrorString(error), file.c_str(), line);
+}
+
+HPM::HPM() {
+    num_images = 0;
+    plane_hypotheses_host = scaled_plane_hypotheses_host = prior_planes_host = nullptr;
+    costs_host = pre_costs_host = confidences_host = texture_host = nullptr;
+    plane_masks_host = nullptr;
+    cameras_cuda = nullptr;
+    texture_objects_cuda = texture_depths_cuda = nullptr;
+    plane_hypotheses_cuda = scaled_plane_hypotheses_cuda = prior_planes_cuda = nullptr;
+    costs_cuda = pre_costs_cuda = depths_cuda = confidences_cuda = texture_cuda = nullptr;
+    rand_states_cuda = nullptr;
+    selected_views_cuda = plane_masks_cuda = Canny_cuda = nullptr;
+    memset(&params, 0, sizeof(params));
+}
+
+HPM::~HPM() {
+    for (int i = 0; i < num_images; ++i) {
+        cudaDestroyTextureObject(texture_objects_host.images[i]);
+        cudaFreeArray(cuArray[i]);
+        if (params.geom_consistency) {
+            cudaDestroyTextureObject(texture_depths_host.images[i]);
+            cudaFreeArray(cuDepthArray[i]);
+        }
+    }
+    delete[] plane_hypotheses_host;
+    delete[] scaled_plane_hypotheses_host;
+    delete[] prior_planes_host;
+    delete[] costs_host;
+    delete[] pre_costs_host;
+    delete[] confidences_host;
+    delete[] texture_host;
+    delete[] plane_masks_host;
+    void* dev[] = {cameras_cuda, texture_objects_cuda, texture_depths_cuda, plane_hypotheses_cuda,
+                   scaled_plane_hypotheses_cuda, prior_planes_cuda, costs_cuda, pre_costs_cuda, depths_cuda,
+                   confidences_cuda, texture_cuda, rand_states_cuda, selected_views_cuda, plane_masks_cuda, Canny_cuda};
+    for (void* d : dev) cudaFree(d);
+}
+
+// plain-C mirror of the PatchMatchParams fields the reference reads
+struct RefParams {
+    int max_iterations, patch_size, num_images, radius_increment;
+    float sigma_spatial, sigma_color;
+    int top_k;
+    float depth_min, depth_max;
+    int scaled_cols, scaled_rows;
+    unsigned int mode;  // hpm_types.h HPM_MODE_* bits
+};
+
+static void make_texture(const float* host, int w, int h, cudaArray** arr, cudaTextureObject_t* tex) {
+    cudaChannelFormatDesc fd = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+    cudaMallocArray(arr, &fd, w, h);
+    cudaMemcpy2DToArray(*arr, 0, 0, host, sizeof(float) * w, sizeof(float) * w, h, cudaMemcpyHostToDevice);
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = *arr;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.addressMode[0] = cudaAddressModeWrap;
+    td.addressMode[1] = cudaAddressModeWrap;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    cudaCreateTextureObject(tex, &rd, &td, nullptr);
+}
+
+extern "C" int ref_run_patchmatch(const float* const* images, const Camera* cams, int num_images, const RefParams* rp,
+                                  float* planes, float* costs, const float* scaled_planes, const float* prior_planes,
+                                  const unsigned int* plane_masks, float* confidences, const unsigned int* canny,
+                                  float* texture, const float* const* depth_maps, unsigned long long seed,
+                                  unsigned int view, float* elapsed_ms) {
+    (void)cudaGetLastError();
+    HPM hpm;
+    const int W = cams[0].width, H = cams[0].height;
+    const size_t n = (size_t)W * H;
+    PatchMatchParams& p = hpm.params;
+    p.max_iterations = rp->max_iterations;
+    p.patch_size = rp->patch_size;
+    p.num_images = num_images;
+    p.radius_increment = rp->radius_increment;
+    p.sigma_spatial = rp->sigma_spatial;
+    p.sigma_color = rp->sigma_color;
+    p.top_k = rp->top_k;
+    p.depth_min = rp->depth_min;
+    p.depth_max = rp->depth_max;
+    p.scaled_cols = (float)rp->scaled_cols;
+    p.scaled_rows = (float)rp->scaled_rows;
+    p.geom_consistency = rp->mode & 1u;
+    p.prior_consistency = rp->mode & 2u;
+    p.multi_geometry = rp->mode & 4u;
+    p.hierarchy = rp->mode & 8u;
+    p.upsample = rp->mode & 16u;
+    p.mand_consistency = rp->mode & 32u;
+    hpm.num_images = num_images;
+    hpm.cameras.assign(cams, cams + num_images);
+    for (int i = 0; i < num_images; ++i)
+        make_texture(images[i], cams[i].width, cams[i].height, &hpm.cuArray[i], &hpm.texture_objects_host.images[i]);
+    cudaMalloc((void**)&hpm.texture_objects_cuda, sizeof(cudaTextureObjects));
+    cudaMemcpy(hpm.texture_objects_cuda, &hpm.texture_objects_host, sizeof(cudaTextureObjects), cudaMemcpyHostToDevice);
+    cudaMalloc((void**)&hpm.cameras_cuda, sizeof(Camera) * num_images);
+    cudaMemcpy(hpm.cameras_cuda, cams, sizeof(Camera) * num_images, cudaMemcpyHostToDevice);
+    hpm.plane_hypotheses_host = new float4[n];
+    memcpy(hpm.plane_hypotheses_host, planes, sizeof(float4) * n);
+    cudaMalloc((void**)&hpm.plane_hypotheses_cuda, sizeof(float4) * n);
+    cudaMemcpy(hpm.plane_hypotheses_cuda, planes, sizeof(float4) * n, cudaMemcpyHostToDevice);
+    hpm.costs_host = new float[n];
+    cudaMalloc((void**)&hpm.costs_cuda, sizeof(float) * n);
+    cudaMemcpy(hpm.costs_cuda, costs, sizeof(float) * n, cudaMemcpyHostToDevice);
+    cudaMalloc((void**)&hpm.pre_costs_cuda, sizeof(float) * n);
+    cudaMalloc((void**)&hpm.rand_states_cuda, sizeof(curandState) * n);
+    cudaMalloc((void**)&hpm.selected_views_cuda, sizeof(unsigned int) * n);
+    cudaMemset(hpm.selected_views_cuda, 0, sizeof(unsigned int) * n);
+    cudaMalloc((void**)&hpm.depths_cuda, sizeof(float) * n);
+    if (p.geom_consistency) {
+        for (int i = 0; i < num_images; ++i)
+            make_texture(depth_maps[i], cams[i].width, cams[i].height, &hpm.cuDepthArray[i],
+                         &hpm.texture_depths_host.images[i]);
+        cudaMalloc((void**)&hpm.texture_depths_cuda, sizeof(cudaTextureObjects));
+        cudaMemcpy(hpm.texture_depths_cuda, &hpm.texture_depths_host, sizeof(cudaTextureObjects), cudaMemcpyHostToDevice);
+    }
+    if (p.hierarchy) {
+        const size_t ns = (size_t)rp->scaled_cols * rp->scaled_rows;
+        hpm.scaled_plane_hypotheses_host = new float4[ns];
+        hpm.pre_costs_host = new float[n];
+        cudaMalloc((void**)&hpm.scaled_plane_hypotheses_cuda, sizeof(float4) * ns);
+        cudaMemcpy(hpm.scaled_plane_hypotheses_cuda, scaled_planes, sizeof(float4) * ns, cudaMemcpyHostToDevice);
+    }
+    if (p.prior_consistency) {
+        hpm.prior_planes_host = new float4[n];
+        hpm.plane_masks_host = new unsigned int[n];
+        cudaMalloc((void**)&hpm.prior_planes_cuda, sizeof(float4) * n);
+        cudaMemcpy(hpm.prior_planes_cuda, prior_planes, sizeof(float4) * n, cudaMemcpyHostToDevice);
+        cudaMalloc((void**)&hpm.plane_masks_cuda, sizeof(unsigned int) * n);
+        cudaMemcpy(hpm.plane_masks_cuda, plane_masks, sizeof(unsigned int) * n, cudaMemcpyHostToDevice);
+    }
+    cudaMalloc((void**)&hpm.confidences_cuda, sizeof(float) * n);
+    cudaMemcpy(hpm.confidences_cuda, confidences, sizeof(float) * n, cudaMemcpyHostToDevice);
+    cudaMalloc((void**)&hpm.Canny_cuda, sizeof(unsigned int) * n);
+    cudaMemcpy(hpm.Canny_cuda, canny, sizeof(unsigned int) * n, cudaMemcpyHostToDevice);
+    hpm.texture_host = new float[n];
+    cudaMalloc((void**)&hpm.texture_cuda, sizeof(float) * n);
+    cudaMemcpyToSymbol(g_ref_seed, &seed, sizeof(seed));
+    cudaMemcpyToSymbol(g_ref_view, &view, sizeof(view));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaDeviceSynchronize();
+    cudaEventRecord(a);
+    hpm.RunPatchMatch();
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (elapsed_ms) *elapsed_ms = ms;
+    memcpy(planes, hpm.plane_hypotheses_host, sizeof(float4) * n);
+    memcpy(costs, hpm.costs_host, sizeof(float) * n);
+    if (!p.mand_consistency && !p.prior_consistency) memcpy(texture, hpm.texture_host, sizeof(float) * n);
+    cudaMemcpy(confidences, hpm.confidences_cuda, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    const cudaError_t err = cudaDeviceSynchronize();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return err == cudaSuccess ? 0 : (int)err;
+}

@@ -1,0 +1,3 @@
+// CHECKER ONLY: see ../cv_stub.hpp
+#pragma once
+#include "../../cv_stub.hpp"

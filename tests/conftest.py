@@ -26,6 +26,8 @@ def _register(name: str, path: str, pkg_dir: str | None = None):
 
 hpm_b200 = _register("hpm_b200", os.path.join(PKG, "__init__.py"), PKG)
 hpm_oracle = _register("hpm_oracle", os.path.join(ROOT, "oracle", "oracle.py"))
+# the oracle pipeline and the reference-build wrapper import `hpm_oracle` by name
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 
 def pytest_configure(config):
