@@ -42,8 +42,20 @@ EXPORTED_SYMBOLS = (
     "hpm_launch_count", "hpm_synchronize", "hpm_sample_view", "hpm_debug_run_partial", "hpm_set_color",
     "hpm_jbu", "hpm_jbu_maps", "hpm_confidence_eval", "hpm_fuse", "hpm_support_points", "hpm_delaunay",
     "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior", "hpm_set_image", "hpm_prepare_level",
-    "hpm_get_level", "hpm_reconstruct", "hpm_get_points",
+    "hpm_get_level", "hpm_reconstruct", "hpm_get_points", "hpm_get_stream", "hpm_profile_enable",
+    "hpm_profile_read", "hpm_measure_fp32_peak",
 )
+
+PROFILE_TIMING = 1
+PROFILE_COUNT = 2
+
+
+class Profile(ctypes.Structure):
+    """hpm_profile: PatchMatch launches, their device time and costed (hypothesis, view) pairs."""
+
+    _fields_ = [("init_launches", ctypes.c_int64), ("sweep_launches", ctypes.c_int64),
+                ("init_ms", ctypes.c_double), ("sweep_ms", ctypes.c_double),
+                ("init_view_evals", ctypes.c_uint64), ("sweep_view_evals", ctypes.c_uint64)]
 
 
 class ReconOptions(ctypes.Structure):
@@ -196,6 +208,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                              ctypes.POINTER(ctypes.c_int64)]
     lib.hpm_debug_run_partial.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int,
                                           ctypes.c_uint64, ctypes.c_int, vp, vp, vp, vp]
+    lib.hpm_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
+    lib.hpm_profile_enable.argtypes = [vp, ctypes.c_int]
+    lib.hpm_profile_read.argtypes = [vp, ctypes.POINTER(Profile)]
+    lib.hpm_measure_fp32_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTED_SYMBOLS:
         getattr(lib, name)
     del i32, f
@@ -268,11 +284,16 @@ class Context:
         h, w = d.shape[:2]
         self._check(self.lib.hpm_set_map(self.h, view, kind, _ptr(d), w, h), "hpm_set_map")
 
-    def get_map(self, view: int, kind: int) -> np.ndarray:
+    def get_map(self, view: int, kind: int, out: np.ndarray | None = None) -> np.ndarray:
+        """Download a map; `out` (float32, C-contiguous, e.g. pinned) receives it when given."""
         w, h = ctypes.c_int(), ctypes.c_int()
         self._check(self.lib.hpm_get_map(self.h, view, kind, None, 0, ctypes.byref(w), ctypes.byref(h)), "hpm_get_map")
         ch = 3 if kind == MAP_NORMAL else 1
-        out = np.empty((h.value, w.value, ch) if ch > 1 else (h.value, w.value), np.float32)
+        shape = (h.value, w.value, ch) if ch > 1 else (h.value, w.value)
+        if out is None:
+            out = np.empty(shape, np.float32)
+        elif out.dtype != np.float32 or not out.flags.c_contiguous or out.size < h.value * w.value * ch:
+            raise HPMError("get_map: `out` must be C-contiguous float32 with room for the map")
         self._check(self.lib.hpm_get_map(self.h, view, kind, _ptr(out), out.size, None, None), "hpm_get_map")
         return out
 
@@ -431,11 +452,16 @@ class Context:
                                              ctypes.byref(n)), "hpm_reconstruct")
         return n.value
 
-    def get_points(self, capacity: int | None = None) -> np.ndarray:
+    def get_points(self, capacity: int | None = None, out: np.ndarray | None = None) -> np.ndarray:
+        """Fused points (n, 9): xyz, normal, colour; `out` (float32 (m, 9), e.g. pinned) receives them."""
         n = ctypes.c_int64()
         self._check(self.lib.hpm_get_points(self.h, None, 0, ctypes.byref(n)), "hpm_get_points")
         cap = n.value if capacity is None else min(capacity, n.value)
-        out = np.zeros((max(cap, 1), 9), np.float32)
+        if out is None:
+            out = np.zeros((max(cap, 1), 9), np.float32)
+        elif out.dtype != np.float32 or not out.flags.c_contiguous or out.ndim != 2 or out.shape[1] != 9:
+            raise HPMError("get_points: `out` must be C-contiguous float32 of shape (m, 9)")
+        cap = min(cap, out.shape[0])
         self._check(self.lib.hpm_get_points(self.h, _ptr(out), cap, None), "hpm_get_points")
         return out[:cap]
 
@@ -444,6 +470,29 @@ class Context:
 
     def launch_count(self) -> int:
         return int(self.lib.hpm_launch_count(self.h))
+
+    def stream_handle(self) -> int:
+        """The cudaStream_t all of this context's work runs on."""
+        s = ctypes.c_void_p()
+        self._check(self.lib.hpm_get_stream(self.h, ctypes.byref(s)), "hpm_get_stream")
+        return int(s.value or 0)
+
+    def profile_enable(self, flags: int) -> None:
+        self._check(self.lib.hpm_profile_enable(self.h, flags), "hpm_profile_enable")
+
+    def profile_read(self) -> Profile:
+        p = Profile()
+        self._check(self.lib.hpm_profile_read(self.h, ctypes.byref(p)), "hpm_profile_read")
+        return p
+
+
+def measure_fp32_peak(device: int = 0) -> float:
+    """FP32 FMA throughput of the device, TFLOP/s (hpm_measure_fp32_peak)."""
+    t = ctypes.c_double()
+    rc = load_library().hpm_measure_fp32_peak(device, ctypes.byref(t))
+    if rc != 0:
+        raise HPMError(f"hpm_measure_fp32_peak failed ({rc})")
+    return t.value
 
 
 @dataclass

@@ -84,6 +84,11 @@ Ctx::~Ctx() {
                      (void*)prior_small, (void*)prior_tris, (void*)prior_label, (void*)prior_work,
                      (void*)prior_unormal, (void*)canny_mag, (void*)canny_grad, (void*)canny_state })
         if (p) cudaFree(p);
+    for (auto& t : prof_events) {
+        cudaEventDestroy(t.start);
+        cudaEventDestroy(t.stop);
+    }
+    if (prof_hyp) cudaFree(prof_hyp);
     if (stream) cudaStreamDestroy(stream);
 }
 

@@ -76,6 +76,16 @@ struct Ctx {
     uint8_t* canny_state = nullptr; size_t canny_state_cap = 0;
     int64_t n_points = 0;
 
+    // profiling (hpm_profile_enable): CUDA events around every PatchMatch
+    // kernel launch, read back and summed by hpm_profile_read
+    int prof_flags = 0;
+    struct TimedLaunch { cudaEvent_t start, stop; int kind; };
+    std::vector<TimedLaunch> prof_events;  // pool; the first prof_used are pending
+    size_t prof_used = 0;
+    unsigned long long* prof_hyp = nullptr;  // device counters [init, sweep]
+    int record_start(int kind, TimedLaunch*& slot);
+    int profile_read(hpm_profile* out);
+
     ~Ctx();
     int fail(int code, const char* fmt, ...);
     int cuda_fail(cudaError_t e, const char* what);

@@ -27,9 +27,12 @@ namespace hpm {
 
 static_assert(sizeof(ViewPoseH) == sizeof(ViewPose), "pose layout");
 
-template <int NS, int BLK>
+// CNT: the counting build of a kernel (profiling); the timed build has it off
+// so the counters do not change its code.
+template <int NS, int BLK, bool CNT = false>
 struct Scratch {
     float* base;  // smem + threadIdx linear
+    static constexpr bool kCount = CNT;
     static constexpr int kWords = 9 * NS + 16;
     __device__ __forceinline__ float& ca(int d, int j) const { return base[(d * NS + j) * BLK]; }
     __device__ __forceinline__ float& vw(int j) const { return base[(8 * NS + j) * BLK]; }
@@ -135,12 +138,13 @@ __device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int 
 
 // ---------------------------------------------------------------- init
 
-template <int NS, int BLK>
+template <int NS, int BLK, bool CNT>
 __device__ float initial_cost(const RunArgs& a, const Patch& P, int px, int py, float4 pl, uint32_t* sel_out,
-                              const Scratch<NS, BLK>& s) {
+                              const Scratch<NS, BLK, CNT>& s) {
     const float cost_max = 2.0f;
     const int S = a.S;
     int valid = 0;
+    if (CNT) atomicAdd(a.hyp_count, (unsigned long long)a.S);
 #pragma unroll 1
     for (int j = 0; j < S; ++j) {
         const float c = ncc_view(a, P, px, py, pl, j);
@@ -180,11 +184,11 @@ __device__ __forceinline__ float range_gauss(float x, float sigma) {
     return (float)exp(-1.0 * (x * x) / (2 * sigma * sigma));
 }
 
-template <int NS, int BLK>
+template <int NS, int BLK, bool CNT>
 __global__ void __launch_bounds__(BLK) k_random_init(const __grid_constant__ RunArgs a) {
     extern __shared__ float smem[];
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    Scratch<NS, BLK> s{ smem + tid };
+    Scratch<NS, BLK, CNT> s{ smem + tid };
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int py = blockIdx.y * blockDim.y + threadIdx.y;
     const int W = a.W, H = a.H;
@@ -295,9 +299,10 @@ __global__ void __launch_bounds__(BLK) k_random_init(const __grid_constant__ Run
 
 // ---------------------------------------------------------------- propagation
 
-template <int NS, int BLK>
+template <int NS, int BLK, bool CNT>
 __device__ __forceinline__ void cost_row(const RunArgs& a, const Patch& P, int px, int py, float4 pl, int d,
-                                         const Scratch<NS, BLK>& s) {
+                                         const Scratch<NS, BLK, CNT>& s) {
+    if (CNT) atomicAdd(a.hyp_count + 1, (unsigned long long)a.S);
 #pragma unroll 1
     for (int j = 0; j < a.S; ++j) s.ca(d, j) = ncc_view(a, P, px, py, pl, j);
 }
@@ -344,9 +349,9 @@ struct CommonOut {
 
 // Direction search, extension, joint view selection and final costs
 // (HPM.cu:1367-1771); shared by both propagation variants.
-template <int NS, int BLK>
+template <int NS, int BLK, bool CNT>
 __device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, int py, int iter, PixelRng& rng,
-                                      const Scratch<NS, BLK>& s) {
+                                      const Scratch<NS, BLK, CNT>& s) {
     const int W = a.W, H = a.H, S = a.S;
     const int center = py * W + px;
     const float* __restrict__ costs = a.costs;
@@ -517,10 +522,11 @@ __device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, 
 }
 
 // Weighted cost of plane pl over the selected views (HPM.cu:1775-1786).
-template <int NS, int BLK>
+template <int NS, int BLK, bool CNT>
 __device__ __forceinline__ float selected_cost(const RunArgs& a, const Patch& P, int px, int py, float4 pl,
-                                               uint32_t selmask, float weight_norm, const Scratch<NS, BLK>& s) {
+                                               uint32_t selmask, float weight_norm, const Scratch<NS, BLK, CNT>& s) {
     const bool geom = a.prm.mode & HPM_MODE_GEOM;
+    if (CNT) atomicAdd(a.hyp_count + 1, (unsigned long long)a.S);
     float c = 0.0f;
 #pragma unroll 1
     for (int j = 0; j < a.S; ++j) {
@@ -559,10 +565,10 @@ __device__ __forceinline__ float prior_score(float final_cost, float depth_now, 
 
 // PlaneHypothesisRefinement (HPM.cu:765-841).  The five candidates are built
 // from the state at entry, evaluated in order and accepted greedily.
-template <int NS, int BLK>
+template <int NS, int BLK, bool CNT>
 __device__ void refinement(const RunArgs& a, const Patch& P, int px, int py, float4& plane, float& depth,
                            float& cost, PixelRng& rng, uint32_t selmask, float weight_norm, float* restricted_cost,
-                           float texture, const Scratch<NS, BLK>& s) {
+                           float texture, const Scratch<NS, BLK, CNT>& s) {
     const hpm_camera& c0 = a.cams[0];
     const int center = py * a.W + px;
     const bool prior = a.prm.mode & HPM_MODE_PRIOR;
@@ -609,11 +615,11 @@ __device__ void refinement(const RunArgs& a, const Patch& P, int px, int py, flo
     }
 }
 
-template <int NS, int BLK, bool MAND>
+template <int NS, int BLK, bool MAND, bool CNT>
 __global__ void __launch_bounds__(BLK) k_half_sweep(const __grid_constant__ RunArgs a, int color, int iter) {
     extern __shared__ float smem[];
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const Scratch<NS, BLK> s{ smem + tid };
+    const Scratch<NS, BLK, CNT> s{ smem + tid };
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int pair = blockIdx.y * blockDim.y + threadIdx.y;
     const int py = 2 * pair + ((px & 1) ^ color);
@@ -634,7 +640,7 @@ __global__ void __launch_bounds__(BLK) k_half_sweep(const __grid_constant__ RunA
     Patch P;
     build_patch(a, px, py, P);
     const bool reliable = MAND ? (a.conf[center] >= 0.3) : true;
-    const CommonOut o = propagate_common<NS, BLK>(a, P, px, py, iter, rng, s);
+    const CommonOut o = propagate_common<NS, BLK, CNT>(a, P, px, py, iter, rng, s);
     float fcl[8];
 #pragma unroll
     for (int d = 0; d < 8; ++d) fcl[d] = s.fc(d);
@@ -800,11 +806,11 @@ __global__ void k_eval_costs(const __grid_constant__ RunArgs a, int n, const int
 template <int NS>
 static constexpr int block_threads() { return NS <= 10 ? 128 : (NS <= 16 ? 64 : 32); }
 
-template <int NS>
+template <int NS, bool CNT>
 static cudaError_t init_impl(const RunArgs& a, cudaStream_t st) {
     constexpr int BLK = 128;
     const size_t shm = sizeof(float) * Scratch<NS, BLK>::kWords * BLK;
-    auto k = k_random_init<NS, BLK>;
+    auto k = k_random_init<NS, BLK, CNT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     if (e != cudaSuccess) return e;
     dim3 block(16, 8), grid((a.W + 15) / 16, (a.H + 7) / 8);
@@ -812,11 +818,11 @@ static cudaError_t init_impl(const RunArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <int NS, bool MAND>
+template <int NS, bool MAND, bool CNT>
 static cudaError_t sweep_impl(const RunArgs& a, int color, int iter, cudaStream_t st) {
     constexpr int BLK = block_threads<NS>();
     const size_t shm = sizeof(float) * Scratch<NS, BLK>::kWords * BLK;
-    auto k = k_half_sweep<NS, BLK, MAND>;
+    auto k = k_half_sweep<NS, BLK, MAND, CNT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     if (e != cudaSuccess) return e;
     dim3 block(32, BLK / 32), grid((a.W + 31) / 32, (a.cover_pairs + BLK / 32 - 1) / (BLK / 32));
@@ -824,19 +830,31 @@ static cudaError_t sweep_impl(const RunArgs& a, int color, int iter, cudaStream_
     return cudaGetLastError();
 }
 
+template <bool CNT>
+static cudaError_t init_dispatch(const RunArgs& a, cudaStream_t st) {
+    if (a.S <= 4) return init_impl<4, CNT>(a, st);
+    if (a.S <= 10) return init_impl<10, CNT>(a, st);
+    if (a.S <= 16) return init_impl<16, CNT>(a, st);
+    return init_impl<31, CNT>(a, st);
+}
+
 cudaError_t launch_random_init(const RunArgs& a, cudaStream_t st) {
-    if (a.S <= 4) return init_impl<4>(a, st);
-    if (a.S <= 10) return init_impl<10>(a, st);
-    if (a.S <= 16) return init_impl<16>(a, st);
-    return init_impl<31>(a, st);
+    return a.hyp_count ? init_dispatch<true>(a, st) : init_dispatch<false>(a, st);
+}
+
+template <bool MAND, bool CNT>
+static cudaError_t sweep_dispatch(const RunArgs& a, int color, int iter, cudaStream_t st) {
+    if (a.S <= 4) return sweep_impl<4, MAND, CNT>(a, color, iter, st);
+    if (a.S <= 10) return sweep_impl<10, MAND, CNT>(a, color, iter, st);
+    if (a.S <= 16) return sweep_impl<16, MAND, CNT>(a, color, iter, st);
+    return sweep_impl<31, MAND, CNT>(a, color, iter, st);
 }
 
 cudaError_t launch_half_sweep(const RunArgs& a, int color, int iter, cudaStream_t st) {
     const bool mand = a.prm.mode & HPM_MODE_MAND;
-    if (a.S <= 4) return mand ? sweep_impl<4, true>(a, color, iter, st) : sweep_impl<4, false>(a, color, iter, st);
-    if (a.S <= 10) return mand ? sweep_impl<10, true>(a, color, iter, st) : sweep_impl<10, false>(a, color, iter, st);
-    if (a.S <= 16) return mand ? sweep_impl<16, true>(a, color, iter, st) : sweep_impl<16, false>(a, color, iter, st);
-    return mand ? sweep_impl<31, true>(a, color, iter, st) : sweep_impl<31, false>(a, color, iter, st);
+    if (a.hyp_count)
+        return mand ? sweep_dispatch<true, true>(a, color, iter, st) : sweep_dispatch<false, true>(a, color, iter, st);
+    return mand ? sweep_dispatch<true, false>(a, color, iter, st) : sweep_dispatch<false, false>(a, color, iter, st);
 }
 
 cudaError_t launch_export(const RunArgs& a, cudaStream_t st) {

@@ -37,6 +37,11 @@ struct RunArgs {
     int S, W, H, cover_pairs;
     uint64_t seed;
     uint32_t view_id;
+    // profiling only (null otherwise): (hypothesis, source view) pairs costed
+    // by [0] the initialisation and [1] the half-sweeps, counted as the
+    // reference evaluates them: every hypothesis against all S sources
+    // (ComputeMultiViewCostVector, HPM.cu:490-495)
+    unsigned long long* hyp_count;
 };
 
 // Host launchers (pm_kernels.cu).  Return cudaError_t of the launch.

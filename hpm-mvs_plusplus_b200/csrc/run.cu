@@ -90,6 +90,7 @@ int Ctx::fill_run_args(int ref, const int32_t* srcs, int n_src, const hpm_params
     a.H = rv.h;
     a.cover_pairs = covered_row_pairs(rv.h);
     a.view_id = (uint32_t)ref;
+    a.hyp_count = (prof_flags & HPM_PROFILE_COUNT) ? prof_hyp : nullptr;
     return HPM_OK;
 }
 
@@ -186,13 +187,59 @@ int Ctx::prepare_run(int ref, const int32_t* srcs, int n_src, const hpm_params* 
     return HPM_OK;
 }
 
+int Ctx::record_start(int kind, TimedLaunch*& slot) {
+    slot = nullptr;
+    if (!(prof_flags & HPM_PROFILE_TIMING)) return HPM_OK;
+    if (prof_used == prof_events.size()) {
+        TimedLaunch t{};
+        cudaError_t e = cudaEventCreate(&t.start);
+        if (e == cudaSuccess) e = cudaEventCreate(&t.stop);
+        if (e != cudaSuccess) return cuda_fail(e, "profiling event");
+        prof_events.push_back(t);
+    }
+    slot = &prof_events[prof_used++];
+    slot->kind = kind;
+    cudaError_t e = cudaEventRecord(slot->start, stream);
+    return e == cudaSuccess ? HPM_OK : cuda_fail(e, "profiling event record");
+}
+
 int Ctx::launch_schedule(const RunArgs& a, int n_half_sweeps) {
     cudaError_t e;
+    TimedLaunch* t = nullptr;
+    int rc = record_start(0, t);
+    if (rc) return rc;
     if ((e = launch_random_init(a, stream)) != cudaSuccess) return cuda_fail(e, "init launch");
+    if (t) cudaEventRecord(t->stop, stream);
     ++launches;
     for (int k = 0; k < n_half_sweeps; ++k) {
+        if ((rc = record_start(1, t))) return rc;
         if ((e = launch_half_sweep(a, k & 1, k >> 1, stream)) != cudaSuccess) return cuda_fail(e, "half sweep");
+        if (t) cudaEventRecord(t->stop, stream);
         ++launches;
+    }
+    return HPM_OK;
+}
+
+int Ctx::profile_read(hpm_profile* out) {
+    cudaSetDevice(device);
+    memset(out, 0, sizeof(*out));
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "profile read");
+    for (size_t i = 0; i < prof_used; ++i) {
+        float ms = 0.0f;
+        e = cudaEventElapsedTime(&ms, prof_events[i].start, prof_events[i].stop);
+        if (e != cudaSuccess) return cuda_fail(e, "profiling event time");
+        if (prof_events[i].kind == 0) { out->init_launches++; out->init_ms += ms; }
+        else { out->sweep_launches++; out->sweep_ms += ms; }
+    }
+    prof_used = 0;
+    if (prof_hyp) {
+        unsigned long long h[2] = {0, 0};
+        e = cudaMemcpy(h, prof_hyp, sizeof(h), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemset(prof_hyp, 0, sizeof(h));
+        if (e != cudaSuccess) return cuda_fail(e, "hypothesis counters");
+        out->init_view_evals = h[0];
+        out->sweep_view_evals = h[1];
     }
     return HPM_OK;
 }

@@ -211,6 +211,37 @@ int64_t hpm_launch_count(const hpm_ctx *ctx);
 /* Wait for all work of the context. */
 int hpm_synchronize(hpm_ctx *ctx);
 
+/* ---- measurement (no reference counterpart; the reference has only its
+ * wall-clock timer, main.cpp:10-23) ---- */
+
+/* The CUDA stream all work of the context is issued on (a cudaStream_t), so a
+ * caller can record its own events around calls. */
+int hpm_get_stream(hpm_ctx *ctx, void **stream);
+
+#define HPM_PROFILE_TIMING 1 /* CUDA events around every PatchMatch kernel launch */
+#define HPM_PROFILE_COUNT 2  /* count (hypothesis, source view) cost evaluations */
+
+typedef struct hpm_profile {
+    int64_t init_launches;     /* random-initialisation launches timed */
+    int64_t sweep_launches;    /* black/red half-sweep launches timed */
+    double init_ms;            /* their summed device time */
+    double sweep_ms;
+    uint64_t init_view_evals;  /* (hypothesis, source view) pairs costed, each 36 patch samples, */
+    uint64_t sweep_view_evals; /*   every hypothesis against all S sources as the reference does */
+} hpm_profile;
+
+/* Turns profiling on (flags) or off (0).  Timing adds two event records per
+ * launch; counting adds one atomic per costed hypothesis. */
+int hpm_profile_enable(hpm_ctx *ctx, int flags);
+
+/* Waits for the context's work, returns what was gathered since the last read
+ * and resets it. */
+int hpm_profile_read(hpm_ctx *ctx, hpm_profile *out);
+
+/* FP32 FMA throughput of the device in TFLOP/s (2 flops per FMA), from a
+ * dependent-chain kernel over all SMs timed with CUDA events. */
+int hpm_measure_fp32_peak(int device, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif
