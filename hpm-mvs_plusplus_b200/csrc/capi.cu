@@ -92,23 +92,6 @@ Ctx::~Ctx() {
     if (stream) cudaStreamDestroy(stream);
 }
 
-// Relative pose of ComputeHomography (HPM.cu:251-279), evaluated on the host
-// in float with the reference's operation order.
-void compute_pose(const hpm_camera& rc, const hpm_camera& sc, ViewPoseH& vp) {
-    float rC[3], sC[3], Cr[3];
-    rC[0] = -(rc.R[0] * rc.t[0] + rc.R[3] * rc.t[1] + rc.R[6] * rc.t[2]);
-    rC[1] = -(rc.R[1] * rc.t[0] + rc.R[4] * rc.t[1] + rc.R[7] * rc.t[2]);
-    rC[2] = -(rc.R[2] * rc.t[0] + rc.R[5] * rc.t[1] + rc.R[8] * rc.t[2]);
-    sC[0] = -(sc.R[0] * sc.t[0] + sc.R[3] * sc.t[1] + sc.R[6] * sc.t[2]);
-    sC[1] = -(sc.R[1] * sc.t[0] + sc.R[4] * sc.t[1] + sc.R[7] * sc.t[2]);
-    sC[2] = -(sc.R[2] * sc.t[0] + sc.R[5] * sc.t[1] + sc.R[8] * sc.t[2]);
-    for (int r = 0; r < 3; ++r)
-        for (int k = 0; k < 3; ++k)
-            vp.Rr[3 * r + k] = sc.R[3 * r] * rc.R[3 * k] + sc.R[3 * r + 1] * rc.R[3 * k + 1] + sc.R[3 * r + 2] * rc.R[3 * k + 2];
-    Cr[0] = rC[0] - sC[0]; Cr[1] = rC[1] - sC[1]; Cr[2] = rC[2] - sC[2];
-    for (int r = 0; r < 3; ++r) vp.tr[r] = sc.R[3 * r] * Cr[0] + sc.R[3 * r + 1] * Cr[1] + sc.R[3 * r + 2] * Cr[2];
-}
-
 // ---------------------------------------------------------------- small kernels
 
 __global__ void k_pack_planes(const float* __restrict__ normal, const float* __restrict__ depth,

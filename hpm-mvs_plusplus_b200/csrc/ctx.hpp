@@ -44,7 +44,6 @@ struct ViewState {
     int color_w = 0, color_h = 0;
 };
 
-void compute_pose(const hpm_camera& rc, const hpm_camera& sc, ViewPoseH& vp);
 
 struct Ctx {
     int device = 0;

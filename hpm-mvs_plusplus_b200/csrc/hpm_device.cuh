@@ -10,6 +10,7 @@
 #include "hpm_types.h"
 #include "hpm_philox.h"
 #include "hpm_fp.h"
+#include "hpm_geometry.h"
 
 namespace hpm {
 
@@ -121,56 +122,6 @@ __device__ __forceinline__ float4 perturbed_normal(const hpm_camera& c, int px, 
     if (np.x * vd.x + np.y * vd.y + np.z * vd.z >= 0.0f) np = normal;
     normalize3(np);
     return np;
-}
-
-// Per source view, the relative pose terms of ComputeHomography (HPM.cu:251-279)
-// that do not depend on the plane.
-struct ViewPose {
-    float Rr[9];
-    float tr[3];
-};
-
-__device__ __forceinline__ void compute_view_pose(const hpm_camera& rc, const hpm_camera& sc, ViewPose& vp) {
-    float rC[3], sC[3], Cr[3];
-    rC[0] = -(rc.R[0] * rc.t[0] + rc.R[3] * rc.t[1] + rc.R[6] * rc.t[2]);
-    rC[1] = -(rc.R[1] * rc.t[0] + rc.R[4] * rc.t[1] + rc.R[7] * rc.t[2]);
-    rC[2] = -(rc.R[2] * rc.t[0] + rc.R[5] * rc.t[1] + rc.R[8] * rc.t[2]);
-    sC[0] = -(sc.R[0] * sc.t[0] + sc.R[3] * sc.t[1] + sc.R[6] * sc.t[2]);
-    sC[1] = -(sc.R[1] * sc.t[0] + sc.R[4] * sc.t[1] + sc.R[7] * sc.t[2]);
-    sC[2] = -(sc.R[2] * sc.t[0] + sc.R[5] * sc.t[1] + sc.R[8] * sc.t[2]);
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-            vp.Rr[3 * r + k] = sc.R[3 * r] * rc.R[3 * k] + sc.R[3 * r + 1] * rc.R[3 * k + 1] + sc.R[3 * r + 2] * rc.R[3 * k + 2];
-    Cr[0] = rC[0] - sC[0]; Cr[1] = rC[1] - sC[1]; Cr[2] = rC[2] - sC[2];
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-        vp.tr[r] = sc.R[3 * r] * Cr[0] + sc.R[3 * r + 1] * Cr[1] + sc.R[3 * r + 2] * Cr[2];
-}
-
-// Plane-induced homography ref -> src (HPM.cu:281-310) from the hoisted pose.
-__device__ __forceinline__ void plane_homography(const hpm_camera& rc, const hpm_camera& sc, const ViewPose& vp,
-                                                 float4 pl, float H[9]) {
-    float Hm[9], tmp[9];
-    const float n[3] = { pl.x, pl.y, pl.z };
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-            Hm[3 * r + k] = vp.Rr[3 * r + k] - vp.tr[r] * n[k] / pl.w;
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        tmp[3 * r + 0] = Hm[3 * r + 0] / rc.K[0];
-        tmp[3 * r + 1] = Hm[3 * r + 1] / rc.K[4];
-        tmp[3 * r + 2] = -Hm[3 * r + 0] * rc.K[2] / rc.K[0] - Hm[3 * r + 1] * rc.K[5] / rc.K[4] + Hm[3 * r + 2];
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        H[0 + k] = sc.K[0] * tmp[0 + k] + sc.K[2] * tmp[6 + k];
-        H[3 + k] = sc.K[4] * tmp[3 + k] + sc.K[5] * tmp[6 + k];
-        H[6 + k] = sc.K[8] * tmp[6 + k];
-    }
 }
 
 __device__ __forceinline__ float3 point_world(float x, float y, float depth, const hpm_camera& c) {

@@ -25,7 +25,6 @@
 
 namespace hpm {
 
-static_assert(sizeof(ViewPoseH) == sizeof(ViewPose), "pose layout");
 
 // CNT: the counting build of a kernel (profiling); the timed build has it off
 // so the counters do not change its code.
@@ -33,11 +32,13 @@ template <int NS, int BLK, bool CNT = false>
 struct Scratch {
     float* base;  // smem + threadIdx linear
     static constexpr bool kCount = CNT;
-    static constexpr int kWords = 9 * NS + 16;
+    // cost rows 0-7 (directions), row 8 (the hypothesis costed against the
+    // selected views), view weights, final costs, candidate positions
+    static constexpr int kWords = 10 * NS + 16;
     __device__ __forceinline__ float& ca(int d, int j) const { return base[(d * NS + j) * BLK]; }
-    __device__ __forceinline__ float& vw(int j) const { return base[(8 * NS + j) * BLK]; }
-    __device__ __forceinline__ float& fc(int d) const { return base[(9 * NS + d) * BLK]; }
-    __device__ __forceinline__ int& pos(int d) const { return reinterpret_cast<int*>(base)[(9 * NS + 8 + d) * BLK]; }
+    __device__ __forceinline__ float& vw(int j) const { return base[(9 * NS + j) * BLK]; }
+    __device__ __forceinline__ float& fc(int d) const { return base[(10 * NS + d) * BLK]; }
+    __device__ __forceinline__ int& pos(int d) const { return reinterpret_cast<int*>(base)[(10 * NS + 8 + d) * BLK]; }
 };
 
 // Statistics of a pixel's reference patch (the view-independent part of the NCC).
@@ -83,14 +84,25 @@ __device__ __forceinline__ void build_patch(const RunArgs& a, int px, int py, Pa
     P.rs.var = s_rr * P.rs.inv_w - P.rs.mean * P.rs.mean;
 }
 
+// m = Kr^-T n / d of a camera-frame hypothesis: the view-independent part of
+// its homographies (include/hpm_geometry.h).
+struct PlaneM {
+    float m[3];
+};
+
+__device__ __forceinline__ PlaneM plane_m(const RunArgs& a, float4 pl) {
+    PlaneM r;
+    hpm_plane_m(a.kinv, pl.x, pl.y, pl.z, pl.w, r.m);
+    return r;
+}
+
 // One bilateral NCC (HPM.cu:375-448) with the patch in registers.
-__device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int px, int py, float4 pl, int j) {
+__device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int px, int py, const PlaneM& pm, int j) {
     const float cost_max = 2.0f;
     if (P.rs.var < 1e-5f) return cost_max;
-    const hpm_camera& rc = a.cams[0];
     const hpm_camera& sc = a.cams[j + 1];
     float H[9];
-    plane_homography(rc, sc, reinterpret_cast<const ViewPose&>(a.pose[j + 1]), pl, H);
+    hpm_homography(a.basis[j + 1].A, a.basis[j + 1].b, pm.m, H);
     const int sw = sc.width, sh = sc.height;
     float iz_c;
     {
@@ -145,9 +157,10 @@ __device__ float initial_cost(const RunArgs& a, const Patch& P, int px, int py, 
     const int S = a.S;
     int valid = 0;
     if (CNT) atomicAdd(a.hyp_count, (unsigned long long)a.S);
+    const PlaneM pm = plane_m(a, pl);
 #pragma unroll 1
     for (int j = 0; j < S; ++j) {
-        const float c = ncc_view(a, P, px, py, pl, j);
+        const float c = ncc_view(a, P, px, py, pm, j);
         s.ca(0, j) = c;
         s.ca(1, j) = c;
         if (c < cost_max) ++valid;
@@ -299,12 +312,15 @@ __global__ void __launch_bounds__(BLK) k_random_init(const __grid_constant__ Run
 
 // ---------------------------------------------------------------- propagation
 
+// Costs of one hypothesis (its PlaneM) against the source views in `mask`,
+// into scratch row `row` (ComputeMultiViewCostVector, HPM.cu:490-495).  The
+// only place a half-sweep evaluates the NCC, so the kernel carries one copy.
 template <int NS, int BLK, bool CNT>
-__device__ __forceinline__ void cost_row(const RunArgs& a, const Patch& P, int px, int py, float4 pl, int d,
-                                         const Scratch<NS, BLK, CNT>& s) {
-    if (CNT) atomicAdd(a.hyp_count + 1, (unsigned long long)a.S);
+__device__ __forceinline__ void eval_row(const RunArgs& a, const Patch& P, int px, int py, const PlaneM& pm,
+                                         uint32_t mask, int row, const Scratch<NS, BLK, CNT>& s) {
 #pragma unroll 1
-    for (int j = 0; j < a.S; ++j) s.ca(d, j) = ncc_view(a, P, px, py, pl, j);
+    for (int j = 0; j < a.S; ++j)
+        if ((mask >> j) & 1u) s.ca(row, j) = ncc_view(a, P, px, py, pm, j);
 }
 
 __device__ __forceinline__ void v_path_scan(const float* __restrict__ costs, int W, int H, int x, int y, int ax,
@@ -340,107 +356,72 @@ __device__ __forceinline__ bool far_search(const float* __restrict__ costs, int 
     return true;
 }
 
-struct CommonOut {
-    uint32_t flags;        // bit d: direction d valid
-    uint32_t temp_selected;
-    int num_selected;
-    float weight_norm;
-};
-
-// Direction search, extension, joint view selection and final costs
-// (HPM.cu:1367-1771); shared by both propagation variants.
+// Non-local candidate positions of the eight directions (HPM.cu:1367-1608);
+// returns the bitmask of valid directions and leaves the positions in scratch.
 template <int NS, int BLK, bool CNT>
-__device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, int py, int iter, PixelRng& rng,
-                                      const Scratch<NS, BLK, CNT>& s) {
-    const int W = a.W, H = a.H, S = a.S;
+__device__ __forceinline__ uint32_t direction_search(const RunArgs& a, int px, int py,
+                                                     const Scratch<NS, BLK, CNT>& s) {
+    const int W = a.W, H = a.H;
     const int center = py * W + px;
     const float* __restrict__ costs = a.costs;
-    const bool geom = a.prm.mode & HPM_MODE_GEOM;
-    CommonOut o;
-    o.flags = 0;
-
-    // `float cost_array[8][32] = { 2.0f }` (HPM.cu:1378): only [0][0] is 2, the rest 0.
-    for (int d = 0; d < 8; ++d)
-        for (int j = 0; j < S; ++j) s.ca(d, j) = 0.0f;
-    s.ca(0, 0) = 2.0f;
-
+    uint32_t flags = 0;
     int pos[8];
     pos[0] = center - 5 - 6 * W; pos[1] = center - 5 * W; pos[2] = center + 6 - 5 * W; pos[3] = center + 5 * W;
     pos[4] = center + 5 + 6 * W; pos[5] = center - 5; pos[6] = center - 6 + 5 * W; pos[7] = center + 5;
-    if (far_search(costs, W, H, px, py, 0, -1, false, pos[1])) o.flags |= 1u << 1;
-    if (far_search(costs, W, H, px, py, 0, 1, false, pos[3])) o.flags |= 1u << 3;
-    if (far_search(costs, W, H, px, py, -1, 0, false, pos[5])) o.flags |= 1u << 5;
-    if (far_search(costs, W, H, px, py, 1, 0, true, pos[7])) o.flags |= 1u << 7;
+    if (far_search(costs, W, H, px, py, 0, -1, false, pos[1])) flags |= 1u << 1;
+    if (far_search(costs, W, H, px, py, 0, 1, false, pos[3])) flags |= 1u << 3;
+    if (far_search(costs, W, H, px, py, -1, 0, false, pos[5])) flags |= 1u << 5;
+    if (far_search(costs, W, H, px, py, 1, 0, true, pos[7])) flags |= 1u << 7;
     if (px > 4 && py > 5) {
-        o.flags |= 1u << 0;
+        flags |= 1u << 0;
         float bc = costs[pos[0]]; int best = pos[0];
         v_path_scan(costs, W, H, px - 5, py - 6, -2, 0, 0, -2, bc, best);
         pos[0] = best;
     }
     if (px < W - 6 && py > 4) {
-        o.flags |= 1u << 2;
+        flags |= 1u << 2;
         float bc = costs[pos[2]]; int best = pos[2];
         v_path_scan(costs, W, H, px + 6, py - 5, 0, -2, 2, 0, bc, best);
         pos[2] = best;
     }
     if (px < W - 5 && py < H - 6) {
-        o.flags |= 1u << 4;
+        flags |= 1u << 4;
         float bc = costs[pos[4]]; int best = pos[4];
         v_path_scan(costs, W, H, px + 5, py + 6, 2, 0, 0, 2, bc, best);
         pos[4] = best;
     }
     if (px > 5 && py < H - 5) {
-        o.flags |= 1u << 6;
+        flags |= 1u << 6;
         float bc = costs[pos[6]]; int best = pos[6];
         v_path_scan(costs, W, H, px - 6, py + 5, 0, 2, -2, 0, bc, best);
         pos[6] = best;
     }
 #pragma unroll
     for (int d = 0; d < 8; ++d) s.pos(d) = pos[d];
+    return flags;
+}
 
-#pragma unroll 1
-    for (int d = 0; d < 8; ++d) {
-        if (o.flags & (1u << d)) cost_row(a, P, px, py, a.planes[s.pos(d)], d, s);
-    }
+struct Selection {
+    uint32_t temp_selected;
+    int num_selected;
+    float weight_norm;
+};
 
-    // Extended propagation: only orientation 0 (left_up) is active because
-    // `bool symbol_eight_orientations[10] = { true }` (HPM.cu:1612, 1063-1126).
-    if (o.flags & 1u) {
-#pragma unroll 1
-        for (int it = 0; it < 3; ++it) {
-            const float good_thr = (float)(0.8 * exp(-iter * iter * (3 - it) / 90.0));
-            int good = 0, bad = 0;
-            for (int j = 0; j < S; ++j) {
-                const float c = s.ca(0, j);
-                if (c < good_thr) ++good;
-                if (c > 1.2f) ++bad;
-            }
-            if (good >= 1 && bad <= 2) break;
-            if (px > 4 + 8 * it && py > 5 + 8 * it) {
-                const int sx = px - 5 - 8 * it, sy = py - 6 - 8 * it;
-                int best = sy * W + sx;
-                float bc = costs[best];
-                v_path_scan(costs, W, H, sx, sy, -2, 0, 0, -2, bc, best);
-                const int prev = s.pos(0);
-                if (bc > costs[prev]) {
-                    best = prev;
-                } else if (best != prev) {
-                    cost_row(a, P, px, py, a.planes[best], 0, s);
-                }
-                // best == prev recomputes the same row in the reference: identical values
-                s.pos(0) = best;
-            }
-        }
-    }
-
-    // Joint view selection (HPM.cu:1686-1751)
+// Joint view selection and the eight final costs (HPM.cu:1686-1771), from the
+// cost rows of the directions; weights to scratch vw, final costs to fc.
+template <int NS, int BLK, bool CNT>
+__device__ __forceinline__ Selection view_selection(const RunArgs& a, int px, int py, int iter, uint32_t flags,
+                                                    PixelRng& rng, const Scratch<NS, BLK, CNT>& s) {
+    const int W = a.W, S = a.S;
+    const int center = py * W + px;
+    const bool geom = a.prm.mode & HPM_MODE_GEOM;
     float priors[NS];
 #pragma unroll
     for (int j = 0; j < NS; ++j) priors[j] = 0.0f;
     const int nbr[4] = { center - W * 5, center + W * 5, center - 5, center + 5 };
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        if (o.flags & (1u << (2 * i + 1))) {
+        if (flags & (1u << (2 * i + 1))) {
             const uint32_t m = a.sel[nbr[i]];
 #pragma unroll
             for (int j = 0; j < NS; ++j)
@@ -486,6 +467,7 @@ __device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, 
             if (!done && j < S && probs[j] > rp) { vw[j] += 1.0f; done = true; }
         }
     }
+    Selection o;
     o.temp_selected = 0; o.num_selected = 0; o.weight_norm = 0.0f;
 #pragma unroll
     for (int j = 0; j < NS; ++j) {
@@ -499,7 +481,7 @@ __device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, 
 #pragma unroll 1
     for (int d = 0; d < 8; ++d) {
         float fc = 0.0f;
-        const bool valid = o.flags & (1u << d);
+        const bool valid = flags & (1u << d);
         float4 pl = make_float4(0.f, 0.f, 0.f, 0.f);
         if (geom && valid) pl = a.planes[s.pos(d)];
         for (int j = 0; j < S; ++j) {
@@ -521,18 +503,18 @@ __device__ CommonOut propagate_common(const RunArgs& a, const Patch& P, int px, 
     return o;
 }
 
-// Weighted cost of plane pl over the selected views (HPM.cu:1775-1786).
+// Weighted cost over the selected views of the hypothesis whose NCCs are in
+// scratch row 8 (HPM.cu:1775-1786, 805-817).
 template <int NS, int BLK, bool CNT>
-__device__ __forceinline__ float selected_cost(const RunArgs& a, const Patch& P, int px, int py, float4 pl,
-                                               uint32_t selmask, float weight_norm, const Scratch<NS, BLK, CNT>& s) {
+__device__ __forceinline__ float selected_cost(const RunArgs& a, int px, int py, float4 pl, uint32_t selmask,
+                                               float weight_norm, const Scratch<NS, BLK, CNT>& s) {
     const bool geom = a.prm.mode & HPM_MODE_GEOM;
-    if (CNT) atomicAdd(a.hyp_count + 1, (unsigned long long)a.S);
     float c = 0.0f;
 #pragma unroll 1
     for (int j = 0; j < a.S; ++j) {
         if (!((selmask >> j) & 1u)) continue;
         const float w = s.vw(j);
-        const float n = ncc_view(a, P, px, py, pl, j);
+        const float n = s.ca(8, j);
         if (geom) c += w * (n + 0.2f * geom_cost(a.depth_src[j + 1], a.dsw[j + 1], a.dsh[j + 1], a.cams[0],
                                                   a.cams[j + 1], pl, px, py));
         else c += w * n;
@@ -563,67 +545,31 @@ __device__ __forceinline__ float prior_score(float final_cost, float depth_now, 
     return (float)(exp(-final_cost * final_cost / beta * (1 + 0.2 * texture)) * (double)prior);
 }
 
-// PlaneHypothesisRefinement (HPM.cu:765-841).  The five candidates are built
-// from the state at entry, evaluated in order and accepted greedily.
-template <int NS, int BLK, bool CNT>
-__device__ void refinement(const RunArgs& a, const Patch& P, int px, int py, float4& plane, float& depth,
-                           float& cost, PixelRng& rng, uint32_t selmask, float weight_norm, float* restricted_cost,
-                           float texture, const Scratch<NS, BLK, CNT>& s) {
-    const hpm_camera& c0 = a.cams[0];
-    const int center = py * a.W + px;
-    const bool prior = a.prm.mode & HPM_MODE_PRIOR;
-    const float perturbation = 0.02f;
-    const float dmin = a.prm.depth_min, dmax = a.prm.depth_max;
-    const float depth_sigma = (dmax - dmin) / 64.0f;
-    const float two_dss = 2 * depth_sigma * depth_sigma;
-    const float angle_sigma = (float)(3.14159265358979323846 * (5.0f / 180.0f));
-    const float two_ass = 2 * angle_sigma * angle_sigma;
-    float depth_prior = 0.0f, depth_rand;
-    float4 plane_rand;
-    const bool use_prior = prior && a.pmask[center] > 0;
-    float4 pp = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (use_prior) {
-        pp = a.prior[center];
-        depth_prior = depth_from_plane(c0, pp, px, py);
-        depth_rand = rng.uniform() * 6 * depth_sigma + (depth_prior - 3 * depth_sigma);
-        plane_rand = perturbed_normal(c0, px, py, pp, rng, angle_sigma);
-    } else {
-        depth_rand = rng.uniform() * (dmax - dmin) + dmin;
-        plane_rand = random_normal(c0, px, py, rng, depth);
-    }
-    const float dmin_p = (1 - perturbation) * depth;
-    const float dmax_p = (1 + perturbation) * depth;
-    const float depth_perturbed = rng.uniform() * (dmax_p - dmin_p) + dmin_p;
-    const float4 plane_perturbed =
-        perturbed_normal(c0, px, py, plane, rng, (float)(perturbation * 3.14159265358979323846));
-    const float depths5[5] = { depth_rand, depth, depth_rand, depth, depth_perturbed };
-    const float4 normals5[5] = { plane, plane_rand, plane_rand, plane_perturbed, plane };
-#pragma unroll 1
-    for (int i = 0; i < 5; ++i) {
-        float4 t = normals5[i];
-        t.w = distance_to_origin(c0, px, py, depths5[i], t);
-        const float tc = selected_cost(a, P, px, py, t, selmask, weight_norm, s);
-        const float db = depth_from_plane(c0, t, px, py);
-        if (use_prior) {
-            const float rt = prior_score(tc, depths5[i], depth_prior, pp, t, texture, two_dss, two_ass);
-            if (db >= dmin && db <= dmax && rt > *restricted_cost) {
-                depth = db; plane = t; cost = tc; *restricted_cost = rt;
-            }
-        } else if (db >= dmin && db <= dmax && tc < cost) {
-            depth = db; plane = t; cost = tc;
-        }
-    }
-}
+// One pixel of a black or red half-sweep: CheckerboardPropagation (HPM.cu:1347-1873)
+// or, with MAND, CheckerboardPropagation_MandatoryConsistency (HPM.cu:1875-2791).
+//
+// The NCC work runs in one loop of 17 slots, each costing at most one
+// hypothesis through eval_row:
+//   slots 0-7    the eight direction candidates, against all sources;
+//   slots 8-10   the three rounds of the left-up extension (HPM.cu:1063-1126);
+//   slot  11     view selection, then the current plane against the selected views;
+//   slots 12-16  the five PlaneHypothesisRefinement candidates (HPM.cu:765-841),
+//                built from the state at entry and accepted greedily in order.
+// The decisions between slots are the reference's, in its order, and the
+// random draws happen in the same sequence.
+#ifndef HPM_SWEEP_MIN_BLOCKS
+#define HPM_SWEEP_MIN_BLOCKS 3  // 3 blocks of 128 threads per SM: at most 170 registers
+#endif
 
 template <int NS, int BLK, bool MAND, bool CNT>
-__global__ void __launch_bounds__(BLK) k_half_sweep(const __grid_constant__ RunArgs a, int color, int iter) {
+__global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const __grid_constant__ RunArgs a, int color, int iter) {
     extern __shared__ float smem[];
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const Scratch<NS, BLK, CNT> s{ smem + tid };
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int pair = blockIdx.y * blockDim.y + threadIdx.y;
     const int py = 2 * pair + ((px & 1) ^ color);
-    const int W = a.W, H = a.H;
+    const int W = a.W, H = a.H, S = a.S;
     if (px >= W || py >= H || pair >= a.cover_pairs) return;
     const int center = py * W + px;
     const hpm_camera& c0 = a.cams[0];
@@ -640,86 +586,244 @@ __global__ void __launch_bounds__(BLK) k_half_sweep(const __grid_constant__ RunA
     Patch P;
     build_patch(a, px, py, P);
     const bool reliable = MAND ? (a.conf[center] >= 0.3) : true;
-    const CommonOut o = propagate_common<NS, BLK, CNT>(a, P, px, py, iter, rng, s);
-    float fcl[8];
-#pragma unroll
-    for (int d = 0; d < 8; ++d) fcl[d] = s.fc(d);
+    const uint32_t all_views = (S >= 32) ? 0xffffffffu : ((1u << S) - 1u);
 
-    if (!MAND || reliable) {
-        const int min_idx = find_min_index8(fcl);
-        const bool min_valid = o.flags & (1u << min_idx);
-        float4 cur = a.planes[center];
-        float cost_now = selected_cost(a, P, px, py, cur, o.temp_selected, o.weight_norm, s);
-        a.costs[center] = cost_now;
-        const float cost_chk = cost_now;  // costs[center] as read by the NaN test
-        float depth_now = depth_from_plane(c0, cur, px, py);
-        float restricted_cost = 0.0f;
-        float texture = 0.0f;
-        float cost_store = cost_now;  // costs[center] before the final write
-        if (!MAND && prior) {
-            const float depth_sigma = (dmax - dmin) / 64.0f;
-            const float two_dss = 2 * depth_sigma * depth_sigma;
-            const float angle_sigma = (float)(3.14159265358979323846 * (5.0f / 180.0f));
-            const float two_ass = 2 * angle_sigma * angle_sigma;
-            const float4 pp = a.prior[center];
-            const float depth_prior = depth_from_plane(c0, pp, px, py);
-            texture = texture_term(a.canny, W, H, px, py);
-            if (a.pmask[center] > 0) {
+    // `float cost_array[8][32] = { 2.0f }` (HPM.cu:1378): only [0][0] is 2, the rest 0.
+    for (int d = 0; d < 8; ++d)
+        for (int j = 0; j < S; ++j) s.ca(d, j) = 0.0f;
+    s.ca(0, 0) = 2.0f;
+    const uint32_t flags = direction_search(a, px, py, s);
+
+    // state carried across slots
+    bool extending = flags & 1u;  // left-up extension still active
+    Selection sel{ 0u, 0, 0.0f };
+    bool refine = false;          // slots 12-16 run
+    bool use_prior = false;
+    float4 cur = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 plane_now = cur;
+    float depth_now = 0.0f, cost_now = 0.0f, restricted_cost = 0.0f, texture = 0.0f, depth_prior = 0.0f;
+    float4 pp = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 plane0 = cur, plane_rand = cur, plane_pert = cur;
+    float depth0 = 0.0f, depth_rand = 0.0f, depth_pert = 0.0f;
+    const float depth_sigma = (dmax - dmin) / 64.0f;
+    const float two_dss = 2 * depth_sigma * depth_sigma;
+    const float angle_sigma = (float)(3.14159265358979323846 * (5.0f / 180.0f));
+    const float two_ass = 2 * angle_sigma * angle_sigma;
+
+#pragma unroll 1
+    for (int t = 0; t < 17; ++t) {
+        bool run = false;
+        float4 pl = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t mask = all_views;
+        int row = 8;
+        if (t < 8) {
+            run = (flags >> t) & 1u;
+            if (run) pl = a.planes[s.pos(t)];
+            row = t;
+        } else if (t < 11) {
+            // Extended propagation: only orientation 0 (left_up) is active because
+            // `bool symbol_eight_orientations[10] = { true }` (HPM.cu:1612, 1063-1126).
+            const int it = t - 8;
+            if (extending) {
+                const float good_thr = (float)(0.8 * exp(-iter * iter * (3 - it) / 90.0));
+                int good = 0, bad = 0;
+                for (int j = 0; j < S; ++j) {
+                    const float c = s.ca(0, j);
+                    if (c < good_thr) ++good;
+                    if (c > 1.2f) ++bad;
+                }
+                if (good >= 1 && bad <= 2) {
+                    extending = false;
+                } else if (px > 4 + 8 * it && py > 5 + 8 * it) {
+                    const int sx = px - 5 - 8 * it, sy = py - 6 - 8 * it;
+                    int best = sy * W + sx;
+                    float bc = a.costs[best];
+                    v_path_scan(a.costs, W, H, sx, sy, -2, 0, 0, -2, bc, best);
+                    const int prev = s.pos(0);
+                    if (bc > a.costs[prev]) {
+                        best = prev;
+                    } else if (best != prev) {
+                        run = true;
+                        pl = a.planes[best];
+                        row = 0;
+                    }
+                    // best == prev recomputes the same row in the reference: identical values
+                    s.pos(0) = best;
+                }
+            }
+        } else if (t == 11) {
+            sel = view_selection(a, px, py, iter, flags, rng, s);
+            cur = a.planes[center];
+            run = true;
+            pl = cur;
+            mask = sel.temp_selected;
+        } else if (refine) {
+            const int i = t - 12;
+            // candidates (depth, normal): (rand, entry) (entry, rand) (rand, rand) (entry, perturbed) (perturbed, entry)
+            pl = (i == 1 || i == 2) ? plane_rand : (i == 3 ? plane_pert : plane0);
+            const float dc = (i == 0 || i == 2) ? depth_rand : (i == 4 ? depth_pert : depth0);
+            pl.w = distance_to_origin(c0, px, py, dc, pl);
+            run = true;
+            mask = sel.temp_selected;
+        }
+
+        if (run) {
+            if (CNT) atomicAdd(a.hyp_count + 1, (unsigned long long)S);
+            const PlaneM pm = plane_m(a, pl);
+            eval_row(a, P, px, py, pm, mask, row, s);
+        }
+
+        if (t == 11) {
+            float fcl[8];
+#pragma unroll
+            for (int d = 0; d < 8; ++d) fcl[d] = s.fc(d);
+            if (!MAND || reliable) {
+                const int min_idx = find_min_index8(fcl);
+                const bool min_valid = flags & (1u << min_idx);
+                cost_now = selected_cost(a, px, py, cur, sel.temp_selected, sel.weight_norm, s);
+                a.costs[center] = cost_now;
+                const float cost_chk = cost_now;  // costs[center] as read by the NaN test
+                depth_now = depth_from_plane(c0, cur, px, py);
+                restricted_cost = 0.0f;
+                texture = 0.0f;
+                if (!MAND && prior) {
+                    pp = a.prior[center];
+                    depth_prior = depth_from_plane(c0, pp, px, py);
+                    texture = texture_term(a.canny, W, H, px, py);
+                    if (a.pmask[center] > 0) {
+                        float rfc[8];
+#pragma unroll
+                        for (int d = 0; d < 8; ++d) {
+                            rfc[d] = 0.0f;
+                            if (flags & (1u << d)) {
+                                const float4 pd = a.planes[s.pos(d)];
+                                const float dn = depth_from_plane(c0, pd, px, py);
+                                rfc[d] = prior_score(fcl[d], dn, depth_prior, pp, pd, texture, two_dss, two_ass);
+                            }
+                        }
+                        const int max_idx = find_max_index8(rfc);
+                        const float rnow = prior_score(cost_now, depth_now, depth_prior, pp, cur, texture, two_dss,
+                                                       two_ass);
+                        if (flags & (1u << max_idx)) {
+                            const float4 pd = a.planes[s.pos(max_idx)];
+                            const float db = depth_from_plane(c0, pd, px, py);
+                            if (db >= dmin && db <= dmax && rfc[max_idx] > rnow) {
+                                depth_now = db;
+                                cur = pd;
+                                a.planes[center] = pd;
+                                a.costs[center] = fcl[max_idx];
+                                restricted_cost = rfc[max_idx];
+                                a.sel[center] = sel.temp_selected;
+                            }
+                        }
+                    } else if (min_valid) {
+                        const float4 pd = a.planes[s.pos(min_idx)];
+                        const float db = depth_from_plane(c0, pd, px, py);
+                        if (db >= dmin && db <= dmax && fcl[min_idx] < cost_now) {
+                            depth_now = db;
+                            cur = pd;
+                            a.planes[center] = pd;
+                            a.costs[center] = fcl[min_idx];
+                        }
+                    }
+                }
+                // plane_hypotheses_now is uninitialised in the reference (HPM.cu:1844, 2299); it
+                // starts as the pixel's current plane here.
+                plane_now = cur;
+                if ((MAND || !prior) && min_valid) {
+                    const float4 pd = a.planes[s.pos(min_idx)];
+                    const float db = depth_from_plane(c0, pd, px, py);
+                    if (db >= dmin && db <= dmax && fcl[min_idx] < cost_now) {
+                        depth_now = db; plane_now = pd; cost_now = fcl[min_idx];
+                        a.sel[center] = sel.temp_selected;
+                    }
+                    if (cost_chk != cost_chk) {
+                        if (!MAND) depth_now = db;
+                        plane_now = pd; cost_now = fcl[min_idx];
+                        a.sel[center] = sel.temp_selected;
+                    }
+                }
+                // PlaneHypothesisRefinement's random draws (HPM.cu:765-799), before any candidate is costed
+                refine = true;
+                use_prior = prior && a.pmask[center] > 0;
+                const float perturbation = 0.02f;
+                if (use_prior) {
+                    depth_rand = rng.uniform() * 6 * depth_sigma + (depth_prior - 3 * depth_sigma);
+                    plane_rand = perturbed_normal(c0, px, py, pp, rng, angle_sigma);
+                } else {
+                    depth_rand = rng.uniform() * (dmax - dmin) + dmin;
+                    plane_rand = random_normal(c0, px, py, rng, depth_now);
+                }
+                const float dmin_p = (1 - perturbation) * depth_now;
+                const float dmax_p = (1 + perturbation) * depth_now;
+                depth_pert = rng.uniform() * (dmax_p - dmin_p) + dmin_p;
+                plane_pert = perturbed_normal(c0, px, py, plane_now, rng,
+                                              (float)(perturbation * 3.14159265358979323846));
+                plane0 = plane_now;
+                depth0 = depth_now;
+            } else {
+                // mandatory consistency, unreliable pixel (HPM.cu:2684-2789)
+                const float beta = 0.18f;
                 float rfc[8];
+                const float mmc = sel.num_selected * 0.5f;
 #pragma unroll
                 for (int d = 0; d < 8; ++d) {
                     rfc[d] = 0.0f;
-                    if (o.flags & (1u << d)) {
-                        const float4 pl = a.planes[s.pos(d)];
-                        const float dn = depth_from_plane(c0, pl, px, py);
-                        rfc[d] = prior_score(fcl[d], dn, depth_prior, pp, pl, texture, two_dss, two_ass);
+                    if (flags & (1u << d)) {
+                        const float cp = a.conf[s.pos(d)];
+                        const float gce = hpm_expf(-fcl[d] * fcl[d] / beta);
+                        const float dm = fmaxf(0.0f, mmc - cp);
+                        const float mce = (float)(0.5f + exp(-dm * dm / (mmc * mmc * 1.0)));
+                        rfc[d] = (cp > 0) ? fmaxf(3.0f, mce) * gce : mce * gce;
+                        if (cp > 0) fcl[d] = (float)(fcl[d] * fmin((double)hpm_expf(-cp * 2), 0.35));
                     }
                 }
                 const int max_idx = find_max_index8(rfc);
-                const float rnow = prior_score(cost_now, depth_now, depth_prior, pp, cur, texture, two_dss, two_ass);
-                if (o.flags & (1u << max_idx)) {
-                    const float4 pl = a.planes[s.pos(max_idx)];
-                    const float db = depth_from_plane(c0, pl, px, py);
+                float cost_u = selected_cost(a, px, py, cur, sel.temp_selected, sel.weight_norm, s);
+                const float cost_chk = cost_u;
+                const float cc = a.conf[center];
+                const float gce = hpm_expf(-cost_u * cost_u / beta);
+                const float dm = fmaxf(0.0f, mmc - cc);
+                const float mce = (float)(0.5f + exp(-dm * dm / (mmc * mmc * 1.0)));
+                const float rnow = (cc > 0) ? fmaxf(3.0f, mce) * gce : mce * gce;
+                if (cc < 0.3) cost_u = (float)(cost_u * exp(0.2 + cc * 2));
+                else cost_u = cost_u * hpm_expf(-cc * 2);
+                float4 pu = cur;  // uninitialised in the reference (HPM.cu:2761)
+                if (flags & (1u << max_idx)) {
+                    const int pm = s.pos(max_idx);
+                    const float4 pd = a.planes[pm];
+                    const float db = depth_from_plane(c0, pd, px, py);
                     if (db >= dmin && db <= dmax && rfc[max_idx] > rnow) {
-                        depth_now = db;
-                        cur = pl;
-                        a.planes[center] = pl;
-                        cost_store = fcl[max_idx];
-                        a.costs[center] = cost_store;
-                        restricted_cost = rfc[max_idx];
-                        a.sel[center] = o.temp_selected;
+                        pu = pd; cost_u = fcl[max_idx];
+                        a.sel[center] = sel.temp_selected;
+                        a.conf[center] = (float)(0.5 * a.conf[pm]);
+                    }
+                    if (cost_chk != cost_chk) {
+                        pu = pd; cost_u = fcl[max_idx];
+                        a.sel[center] = sel.temp_selected;
+                        a.conf[center] = (float)(0.5 * a.conf[pm]);
                     }
                 }
-            } else if (min_valid) {
-                const float4 pl = a.planes[s.pos(min_idx)];
-                const float db = depth_from_plane(c0, pl, px, py);
-                if (db >= dmin && db <= dmax && fcl[min_idx] < cost_now) {
-                    depth_now = db;
-                    cur = pl;
-                    a.planes[center] = pl;
-                    cost_store = fcl[min_idx];
-                    a.costs[center] = cost_store;
-                }
+                a.costs[center] = cost_u;
+                a.planes[center] = pu;
             }
-        }
-        // plane_hypotheses_now is uninitialised in the reference (HPM.cu:1844, 2299); it
-        // starts as the pixel's current plane here.
-        float4 plane_now = cur;
-        if ((MAND || !prior) && min_valid) {
-            const float4 pl = a.planes[s.pos(min_idx)];
+        } else if (t >= 12 && refine) {
+            const int i = t - 12;
+            const float dc = (i == 0 || i == 2) ? depth_rand : (i == 4 ? depth_pert : depth0);
+            const float tc = selected_cost(a, px, py, pl, sel.temp_selected, sel.weight_norm, s);
             const float db = depth_from_plane(c0, pl, px, py);
-            if (db >= dmin && db <= dmax && fcl[min_idx] < cost_now) {
-                depth_now = db; plane_now = pl; cost_now = fcl[min_idx];
-                a.sel[center] = o.temp_selected;
-            }
-            if (cost_chk != cost_chk) {
-                if (!MAND) depth_now = db;
-                plane_now = pl; cost_now = fcl[min_idx];
-                a.sel[center] = o.temp_selected;
+            if (use_prior) {
+                const float rt = prior_score(tc, dc, depth_prior, pp, pl, texture, two_dss, two_ass);
+                if (db >= dmin && db <= dmax && rt > restricted_cost) {
+                    depth_now = db; plane_now = pl; cost_now = tc; restricted_cost = rt;
+                }
+            } else if (db >= dmin && db <= dmax && tc < cost_now) {
+                depth_now = db; plane_now = pl; cost_now = tc;
             }
         }
-        refinement(a, P, px, py, plane_now, depth_now, cost_now, rng, o.temp_selected, o.weight_norm,
-                   &restricted_cost, texture, s);
+    }
+
+    if (refine) {
         if (!MAND && hier) {
             if (cost_now < a.pre_costs[center] - 0.1f) {
                 a.costs[center] = cost_now;
@@ -729,53 +833,6 @@ __global__ void __launch_bounds__(BLK) k_half_sweep(const __grid_constant__ RunA
             a.costs[center] = cost_now;
             a.planes[center] = plane_now;
         }
-        (void)cost_store;
-    } else {
-        // mandatory consistency, unreliable pixel (HPM.cu:2684-2789)
-        const float beta = 0.18f;
-        float rfc[8];
-        const float mmc = o.num_selected * 0.5f;
-#pragma unroll
-        for (int d = 0; d < 8; ++d) {
-            rfc[d] = 0.0f;
-            if (o.flags & (1u << d)) {
-                const float cp = a.conf[s.pos(d)];
-                const float gce = hpm_expf(-fcl[d] * fcl[d] / beta);
-                const float dm = fmaxf(0.0f, mmc - cp);
-                const float mce = (float)(0.5f + exp(-dm * dm / (mmc * mmc * 1.0)));
-                rfc[d] = (cp > 0) ? fmaxf(3.0f, mce) * gce : mce * gce;
-                if (cp > 0) fcl[d] = (float)(fcl[d] * fmin((double)hpm_expf(-cp * 2), 0.35));
-            }
-        }
-        const int max_idx = find_max_index8(rfc);
-        const float4 cur = a.planes[center];
-        float cost_now = selected_cost(a, P, px, py, cur, o.temp_selected, o.weight_norm, s);
-        const float cost_chk = cost_now;
-        const float cc = a.conf[center];
-        const float gce = hpm_expf(-cost_now * cost_now / beta);
-        const float dm = fmaxf(0.0f, mmc - cc);
-        const float mce = (float)(0.5f + exp(-dm * dm / (mmc * mmc * 1.0)));
-        const float rnow = (cc > 0) ? fmaxf(3.0f, mce) * gce : mce * gce;
-        if (cc < 0.3) cost_now = (float)(cost_now * exp(0.2 + cc * 2));
-        else cost_now = cost_now * hpm_expf(-cc * 2);
-        float4 plane_now = cur;  // uninitialised in the reference (HPM.cu:2761)
-        if (o.flags & (1u << max_idx)) {
-            const int pm = s.pos(max_idx);
-            const float4 pl = a.planes[pm];
-            const float db = depth_from_plane(c0, pl, px, py);
-            if (db >= dmin && db <= dmax && rfc[max_idx] > rnow) {
-                plane_now = pl; cost_now = fcl[max_idx];
-                a.sel[center] = o.temp_selected;
-                a.conf[center] = (float)(0.5 * a.conf[pm]);
-            }
-            if (cost_chk != cost_chk) {
-                plane_now = pl; cost_now = fcl[max_idx];
-                a.sel[center] = o.temp_selected;
-                a.conf[center] = (float)(0.5 * a.conf[pm]);
-            }
-        }
-        a.costs[center] = cost_now;
-        a.planes[center] = plane_now;
     }
     a.rng[center] = rng.draw;
 }
@@ -798,7 +855,8 @@ __global__ void k_eval_costs(const __grid_constant__ RunArgs a, int n, const int
     Patch P;
     build_patch(a, x, y, P);
     const float4 pl = planes[k];
-    for (int j = 0; j < a.S; ++j) out[(size_t)k * a.S + j] = ncc_view(a, P, x, y, pl, j);
+    const PlaneM pm = plane_m(a, pl);
+    for (int j = 0; j < a.S; ++j) out[(size_t)k * a.S + j] = ncc_view(a, P, x, y, pm, j);
 }
 
 // ---------------------------------------------------------------- launchers

@@ -8,16 +8,19 @@
 
 namespace hpm {
 
-struct ViewPoseH {  // host mirror of ViewPose (same layout)
-    float Rr[9];
-    float tr[3];
+// Per-view basis of the plane-induced homography H = A - b m^T
+// (include/hpm_geometry.h, ComputeHomography HPM.cu:251-311).
+struct ViewBasis {
+    float A[9];
+    float b[3];
 };
 
 // Everything one PatchMatch run of one reference view reads.  Passed by value
 // as a __grid_constant__ kernel parameter (about 6 KB).
 struct RunArgs {
     hpm_camera cams[32];            // 0 = reference
-    ViewPoseH pose[32];             // relative pose of source j+1 w.r.t. the reference
+    ViewBasis basis[32];            // homography basis of source j+1 w.r.t. the reference
+    float kinv[4];                  // 1/fx, 1/fy, cx/fx, cy/fy of the reference camera
     cudaTextureObject_t tex[32];    // linear-filtered source images (index j+1)
     const float* depth_src[32];     // geometric mode: source depth maps (index j+1)
     int dsw[32], dsh[32];           // their sizes

@@ -3,6 +3,7 @@
 // (HPM.cpp:741-906, 942-984), HPM::RunPatchMatch (HPM.cu:2987-3035) and the
 // result hand-off of ProcessProblem (main.cpp:599-626).
 #include "ctx.hpp"
+#include "hpm_geometry.h"
 #include "pm_kernels.cuh"
 #include "aux_kernels.cuh"
 
@@ -81,8 +82,9 @@ int Ctx::fill_run_args(int ref, const int32_t* srcs, int n_src, const hpm_params
         if (s < 0 || s >= HPM_MAX_VIEWS || views[s].w == 0) return fail(HPM_E_STATE, "source view %d not set", s);
         a.cams[j + 1] = views[s].cam;
         a.tex[j + 1] = views[s].tex;
-        compute_pose(rv.cam, views[s].cam, a.pose[j + 1]);
+        hpm_view_basis(&rv.cam, &views[s].cam, a.basis[j + 1].A, a.basis[j + 1].b);
     }
+    hpm_ref_kinv(&rv.cam, a.kinv);
     a.ref_img = rv.gray;
     a.prm = *params;
     a.S = n_src;

@@ -14,6 +14,7 @@
 #include "hpm_oracle.h"
 #include "hpm_philox.h"
 #include "hpm_fp.h"
+#include "hpm_geometry.h"
 
 #include <float.h>
 #include <math.h>
@@ -157,37 +158,6 @@ static f4 rotate_to_cam(const hpm_camera *c, f4 p) /* TransformNormal2RefCam, HP
     return r;
 }
 
-static void homography(const hpm_camera *rc, const hpm_camera *sc, f4 pl, float H[9])
-{
-    float rC[3], sC[3], Rr[9], Cr[3], tr[3], tmp[9];
-    rC[0] = -(rc->R[0] * rc->t[0] + rc->R[3] * rc->t[1] + rc->R[6] * rc->t[2]);
-    rC[1] = -(rc->R[1] * rc->t[0] + rc->R[4] * rc->t[1] + rc->R[7] * rc->t[2]);
-    rC[2] = -(rc->R[2] * rc->t[0] + rc->R[5] * rc->t[1] + rc->R[8] * rc->t[2]);
-    sC[0] = -(sc->R[0] * sc->t[0] + sc->R[3] * sc->t[1] + sc->R[6] * sc->t[2]);
-    sC[1] = -(sc->R[1] * sc->t[0] + sc->R[4] * sc->t[1] + sc->R[7] * sc->t[2]);
-    sC[2] = -(sc->R[2] * sc->t[0] + sc->R[5] * sc->t[1] + sc->R[8] * sc->t[2]);
-    for (int r = 0; r < 3; ++r)
-        for (int k = 0; k < 3; ++k)
-            Rr[3 * r + k] = sc->R[3 * r + 0] * rc->R[3 * k + 0] + sc->R[3 * r + 1] * rc->R[3 * k + 1] + sc->R[3 * r + 2] * rc->R[3 * k + 2];
-    Cr[0] = rC[0] - sC[0]; Cr[1] = rC[1] - sC[1]; Cr[2] = rC[2] - sC[2];
-    for (int r = 0; r < 3; ++r)
-        tr[r] = sc->R[3 * r + 0] * Cr[0] + sc->R[3 * r + 1] * Cr[1] + sc->R[3 * r + 2] * Cr[2];
-    const float n[3] = { pl.x, pl.y, pl.z };
-    for (int r = 0; r < 3; ++r)
-        for (int k = 0; k < 3; ++k)
-            H[3 * r + k] = Rr[3 * r + k] - tr[r] * n[k] / pl.w;
-    for (int r = 0; r < 3; ++r) {
-        tmp[3 * r + 0] = H[3 * r + 0] / rc->K[0];
-        tmp[3 * r + 1] = H[3 * r + 1] / rc->K[4];
-        tmp[3 * r + 2] = -H[3 * r + 0] * rc->K[2] / rc->K[0] - H[3 * r + 1] * rc->K[5] / rc->K[4] + H[3 * r + 2];
-    }
-    for (int k = 0; k < 3; ++k) {
-        H[0 + k] = sc->K[0] * tmp[0 + k] + sc->K[2] * tmp[6 + k];
-        H[3 + k] = sc->K[4] * tmp[3 + k] + sc->K[5] * tmp[6 + k];
-        H[6 + k] = sc->K[8] * tmp[6 + k];
-    }
-}
-
 static inline f2 corresponding_point(const float H[9], int x, int y)
 {
     const float px = H[0] * x + H[1] * y + H[2];
@@ -307,9 +277,12 @@ float ora_bilateral_ncc(const float *ref, const hpm_camera *rc, const float *src
     const float kMinVar = 1e-5f;
     if (var_r < kMinVar) return cost_max;
 
-    const f4 pl = { plane[0], plane[1], plane[2], plane[3] };
-    float H[9];
-    homography(rc, sc, pl, H);
+    /* homography factored as H = A - b m^T (include/hpm_geometry.h) */
+    float A[9], bv[3], kinv[4], m[3], H[9];
+    hpm_view_basis(rc, sc, A, bv);
+    hpm_ref_kinv(rc, kinv);
+    hpm_plane_m(kinv, plane[0], plane[1], plane[2], plane[3], m);
+    hpm_homography(A, bv, m, H);
     float iz_c;
     {
         const float fx = (float)px, fy = (float)py;
