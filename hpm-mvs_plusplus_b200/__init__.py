@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "hpm_jbu", "hpm_jbu_maps", "hpm_confidence_eval", "hpm_fuse", "hpm_support_points", "hpm_delaunay",
     "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior", "hpm_set_image", "hpm_prepare_level",
     "hpm_get_level", "hpm_reconstruct", "hpm_get_points", "hpm_get_stream", "hpm_profile_enable",
-    "hpm_profile_read", "hpm_measure_fp32_peak",
+    "hpm_profile_read", "hpm_measure_fp32_peak", "hpm_eval_costs_noalloc",
 )
 
 PROFILE_TIMING = 1
@@ -183,6 +183,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                        ctypes.c_uint64]
     lib.hpm_eval_costs.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int, vp, vp,
                                    vp]
+    lib.hpm_eval_costs_noalloc.argtypes = lib.hpm_eval_costs.argtypes
     lib.hpm_set_address_mode.argtypes = [vp, ctypes.c_int]
     lib.hpm_launch_count.argtypes = [vp]
     lib.hpm_launch_count.restype = ctypes.c_int64
@@ -322,6 +323,18 @@ class Context:
         out = np.empty((p.shape[0], len(s)), np.float32)
         self._check(self.lib.hpm_eval_costs(self.h, ref, _ptr(s), len(s), ctypes.byref(params), p.shape[0], _ptr(p),
                                             _ptr(pl), _ptr(out)), "hpm_eval_costs")
+        return out
+
+    def eval_costs_noalloc(self, ref: int, srcs: Sequence[int], params: Params, px: np.ndarray,
+                           planes: np.ndarray) -> np.ndarray:
+        """eval_costs for callers that cannot have the library allocate device memory while they run
+        (hpm_eval_costs_noalloc: fixed 4 MiB of staging per GPU, n * (24 + 4 * len(srcs)) bytes per call)."""
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        p = np.ascontiguousarray(px, dtype=np.int32).reshape(-1, 2)
+        pl = np.ascontiguousarray(planes, dtype=np.float32).reshape(-1, 4)
+        out = np.empty((p.shape[0], len(s)), np.float32)
+        self._check(self.lib.hpm_eval_costs_noalloc(self.h, ref, _ptr(s), len(s), ctypes.byref(params), p.shape[0],
+                                                    _ptr(p), _ptr(pl), _ptr(out)), "hpm_eval_costs_noalloc")
         return out
 
     def sample_view(self, view: int, xy: np.ndarray) -> np.ndarray:

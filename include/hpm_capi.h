@@ -105,6 +105,18 @@ int hpm_run_patchmatch(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, co
 int hpm_eval_costs(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, const hpm_params *params, int n,
                    const int32_t *px, const float *planes, float *out);
 
+/* hpm_eval_costs without any device allocation.  No counterpart in the
+ * reference.  For callers that must not have cudaMalloc/cudaFree run under them
+ * (those calls can synchronise the whole device and can fail when the process's
+ * device memory is owned by another allocator with a fixed budget).  Same
+ * arguments and results as hpm_eval_costs; the device staging lives in one
+ * fixed 4 MiB array per GPU, so n * (24 + 4 * n_src) bytes (plus alignment)
+ * must fit, else HPM_E_INVALID.  All calls on a device share that array: calls
+ * that overlap on the GPU race.  The first call on a device looks up the
+ * array's address; make it before any stream capture. */
+int hpm_eval_costs_noalloc(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, const hpm_params *params, int n,
+                           const int32_t *px, const float *planes, float *out);
+
 /* Colour image (BGR, 8 bits) of a view at the size of its maps, for the point
  * colours of fusion (the rescaled image of RunFusion, main.cpp:863-865). */
 int hpm_set_color(hpm_ctx *ctx, int view, const uint8_t *bgr, int w, int h);
