@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = (
     "hpm_jbu", "hpm_jbu_maps", "hpm_confidence_eval", "hpm_fuse", "hpm_support_points", "hpm_delaunay",
     "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior", "hpm_set_image", "hpm_prepare_level",
     "hpm_get_level", "hpm_reconstruct", "hpm_get_points", "hpm_get_stream", "hpm_profile_enable",
-    "hpm_profile_read", "hpm_measure_fp32_peak", "hpm_eval_costs_noalloc",
+    "hpm_profile_read", "hpm_measure_fp32_peak", "hpm_eval_costs_noalloc", "hpm_eval_cost_grad", "hpm_gn_refine",
 )
 
 PROFILE_TIMING = 1
@@ -184,6 +184,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.hpm_eval_costs.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int, vp, vp,
                                    vp]
     lib.hpm_eval_costs_noalloc.argtypes = lib.hpm_eval_costs.argtypes
+    lib.hpm_eval_cost_grad.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int, vp,
+                                       vp, vp, vp]
+    lib.hpm_gn_refine.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int,
+                                  ctypes.c_int]
     lib.hpm_set_address_mode.argtypes = [vp, ctypes.c_int]
     lib.hpm_launch_count.argtypes = [vp]
     lib.hpm_launch_count.restype = ctypes.c_int64
@@ -336,6 +340,26 @@ class Context:
         self._check(self.lib.hpm_eval_costs_noalloc(self.h, ref, _ptr(s), len(s), ctypes.byref(params), p.shape[0],
                                                     _ptr(p), _ptr(pl), _ptr(out)), "hpm_eval_costs_noalloc")
         return out
+
+    def eval_cost_grad(self, ref: int, srcs: Sequence[int], params: Params, px: np.ndarray, theta: np.ndarray,
+                       with_grad: bool = True):
+        """Differentiable costs (n, S) and d cost / d (depth, nx, ny) (n, S, 3) (hpm_eval_cost_grad)."""
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        p = np.ascontiguousarray(px, dtype=np.int32).reshape(-1, 2)
+        th = np.ascontiguousarray(theta, dtype=np.float32).reshape(-1, 3)
+        cost = np.empty((p.shape[0], len(s)), np.float32)
+        grad = np.empty((p.shape[0], len(s), 3), np.float32) if with_grad else None
+        self._check(self.lib.hpm_eval_cost_grad(self.h, ref, _ptr(s), len(s), ctypes.byref(params), p.shape[0],
+                                                _ptr(p), _ptr(th), _ptr(cost), _ptr(grad) if with_grad else None),
+                    "hpm_eval_cost_grad")
+        return cost, grad
+
+    def gn_refine(self, ref: int, srcs: Sequence[int], params: Params, depth_kind: int = MAP_DEPTH_GEOM,
+                  steps: int = 3) -> None:
+        """Gauss-Newton refinement of the view's resident depth/normal maps (hpm_gn_refine)."""
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        self._check(self.lib.hpm_gn_refine(self.h, ref, _ptr(s), len(s), ctypes.byref(params), depth_kind, steps),
+                    "hpm_gn_refine")
 
     def sample_view(self, view: int, xy: np.ndarray) -> np.ndarray:
         c = np.ascontiguousarray(xy, dtype=np.float32).reshape(-1, 2)

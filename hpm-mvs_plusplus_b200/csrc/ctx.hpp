@@ -45,6 +45,8 @@ struct ViewState {
 };
 
 
+struct SrcImages;
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -113,6 +115,11 @@ struct Ctx {
     int canny_view(int view);
     int reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off, const int32_t* src_ids,
                     const hpm_recon_options* opt, int64_t* n_points_out);
+    cudaError_t ensure_scratch(size_t bytes);
+    int fill_src_images(const int32_t* srcs, int n_src, SrcImages& si);
+    int eval_cost_grad(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n, const int32_t* px,
+                       const float* theta, float* cost, float* grad);
+    int gn_refine(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int depth_kind, int steps);
     int eval_costs(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n, const int32_t* px,
                    const float* planes, float* out);
 };

@@ -7,10 +7,15 @@
 #include "ctx.hpp"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <future>
+#include <thread>
 #include <vector>
 
 namespace hpm {
+
+int delaunay_triangulate(const int32_t* xy, int n, int width, int height, std::vector<hpm_triangle>& out);
 
 namespace {
 
@@ -76,20 +81,47 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
     auto confidence = [&](int depth_kind) -> int {
         return consistency_scan(0, n_views, src_off, src_ids, depth_kind, nullptr, nullptr, 0, nullptr, nullptr);
     };
+    // A view's prior depends only on its own maps and the confidences computed
+    // before the pass, so all support points are taken first and the host
+    // triangulations run on worker threads while the GPU works through the
+    // views in order (view i's PatchMatch overlaps the triangulation of later
+    // views).  The results are those of one view at a time.
     auto prior_passes = [&](int level) -> int {
         for (int hpm_scale = max_hpm_scale; hpm_scale >= level; --hpm_scale) {
             int r = confidence(HPM_MAP_DEPTH);
             if (r) return r;
             ++pass;
+            std::vector<std::vector<int32_t>> xy(n_views);
+            std::vector<int> sup_w(n_views), sup_h(n_views), dist(n_views);
             for (int i = 0; i < n_views; ++i) {
-                const int distance = hpm_scale - num_downscale[i] - 1;
-                if (distance < 0 || distance > 2)
-                    return fail(HPM_E_STATE, "view %d: prior scale distance %d is outside 0..2", i, distance);
-                r = build_prior(i, distance, nullptr, nullptr);
-                if (r) return r;
-                r = run(i, HPM_MODE_PRIOR, level);
+                dist[i] = hpm_scale - num_downscale[i] - 1;
+                if (dist[i] < 0 || dist[i] > 2)
+                    return fail(HPM_E_STATE, "view %d: prior scale distance %d is outside 0..2", i, dist[i]);
+                if (!views[i].maps[HPM_MAP_DEPTH].ptr) return fail(HPM_E_STATE, "view %d lacks a depth map", i);
+                r = support_points(i, dist[i], xy[i], sup_w[i], sup_h[i]);
                 if (r) return r;
             }
+            std::vector<std::future<std::vector<hpm_triangle>>> tris(n_views);
+            const int workers = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+            std::atomic<int> next{ 0 };
+            std::vector<std::promise<std::vector<hpm_triangle>>> done(n_views);
+            for (int i = 0; i < n_views; ++i) tris[i] = done[i].get_future();
+            std::vector<std::thread> pool;
+            for (int w = 0; w < std::min(workers, n_views); ++w)
+                pool.emplace_back([&]() {
+                    for (int i = next++; i < n_views; i = next++) {
+                        std::vector<hpm_triangle> t;
+                        delaunay_triangulate(xy[i].data(), (int)xy[i].size() / 2, sup_w[i], sup_h[i], t);
+                        done[i].set_value(std::move(t));
+                    }
+                });
+            for (int i = 0; i < n_views && !r; ++i) {
+                const std::vector<hpm_triangle> t = tris[i].get();
+                r = prior_from_triangles(i, dist[i], t.data(), (int)t.size(), sup_w[i], sup_h[i]);
+                if (!r) r = run(i, HPM_MODE_PRIOR, level);
+            }
+            for (auto& th : pool) th.join();
+            if (r) return r;
         }
         return HPM_OK;
     };

@@ -315,6 +315,10 @@ __global__ void __launch_bounds__(BLK) k_random_init(const __grid_constant__ Run
 // Costs of one hypothesis (its PlaneM) against the source views in `mask`,
 // into scratch row `row` (ComputeMultiViewCostVector, HPM.cu:490-495).  The
 // only place a half-sweep evaluates the NCC, so the kernel carries one copy.
+// The loop runs over view indices, the same for every lane: a variant in which
+// each lane took its own k-th selected view ran three times slower on B200,
+// because texture fetches with different texture objects across a warp
+// serialise.
 template <int NS, int BLK, bool CNT>
 __device__ __forceinline__ void eval_row(const RunArgs& a, const Patch& P, int px, int py, const PlaneM& pm,
                                          uint32_t mask, int row, const Scratch<NS, BLK, CNT>& s) {

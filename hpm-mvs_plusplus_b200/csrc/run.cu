@@ -350,6 +350,8 @@ int Ctx::jbu_view(int view, int* applied) {
     return HPM_OK;
 }
 
+cudaError_t Ctx::ensure_scratch(size_t bytes) { return ensure_buf(scratch, scratch_cap, bytes); }
+
 int Ctx::eval_costs(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n, const int32_t* px,
                     const float* planes_h, float* out) {
     cudaSetDevice(device);

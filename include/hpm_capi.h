@@ -117,6 +117,27 @@ int hpm_eval_costs(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, const 
 int hpm_eval_costs_noalloc(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, const hpm_params *params, int n,
                            const int32_t *px, const float *planes, float *out);
 
+/* Differentiable form of the bilateral NCC (HPM.cu:375-448 with exact
+ * bilinear sampling of the sources) and its adjoint; no counterpart in the
+ * reference.  For n (pixel, hypothesis) pairs, theta[3k..3k+2] = (depth, nx,
+ * ny) in the reference camera frame with nz = -sqrt(1 - nx^2 - ny^2):
+ * cost[k*n_src + j] and, when grad is not null, grad[(k*n_src + j)*3 + a] =
+ * d cost / d theta_a.  Costs of 2 (out-of-image centre, flat patch) and
+ * clamped costs have zero gradient.  The warped samples are recomputed, not
+ * stored. */
+int hpm_eval_cost_grad(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, const hpm_params *params, int n,
+                       const int32_t *px, const float *theta, float *cost, float *grad);
+
+/* Gauss-Newton refinement of a view's resident planes (no counterpart in the
+ * reference, where refinement is PlaneHypothesisRefinement's random
+ * perturbations, HPM.cu:765-841): `steps` damped Gauss-Newton steps per pixel
+ * on the sum of squared costs of hpm_eval_cost_grad over the sources whose
+ * cost starts in (0, 2), updating the view's `depth_kind` (DEPTH or
+ * DEPTH_GEOM) and NORMAL maps in place and writing the RMS cost to COST.
+ * Depths stay in params' [depth_min, depth_max]. */
+int hpm_gn_refine(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, const hpm_params *params, int depth_kind,
+                  int steps);
+
 /* Colour image (BGR, 8 bits) of a view at the size of its maps, for the point
  * colours of fusion (the rescaled image of RunFusion, main.cpp:863-865). */
 int hpm_set_color(hpm_ctx *ctx, int view, const uint8_t *bgr, int w, int h);

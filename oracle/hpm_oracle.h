@@ -163,6 +163,13 @@ float ora_uniform(uint64_t seed, uint32_t view, uint32_t x, uint32_t y, uint32_t
 /* cv::resize INTER_LINEAR for a single-channel float image. */
 void ora_resize_linear_f32(const float *src, int sw, int sh, float *dst, int dw, int dh);
 
+/* FP64 differentiable bilateral NCC of pixel (px, py) under the camera-frame
+ * plane theta = (depth, nx, ny), nz = -sqrt(1 - nx^2 - ny^2), against one
+ * source view (exact bilinear sampling); returns the cost and, when grad is
+ * not null, d cost / d theta (hpm_oracle_grad.c). */
+double ora_cost_grad64(const float *ref, const hpm_camera *rc, const float *src, const hpm_camera *sc,
+                       const hpm_params *prm, int px, int py, const double theta[3], double grad[3]);
+
 #ifdef __cplusplus
 }
 #endif

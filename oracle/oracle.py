@@ -97,6 +97,9 @@ def lib() -> ctypes.CDLL:
         L.ora_philox.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp]
         L.ora_prior_reload.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(Camera), ctypes.c_float,
                                        ctypes.c_float, vp, vp]
+        L.ora_cost_grad64.restype = ctypes.c_double
+        L.ora_cost_grad64.argtypes = [vp, ctypes.POINTER(Camera), vp, ctypes.POINTER(Camera), ctypes.POINTER(Params),
+                                      ctypes.c_int, ctypes.c_int, vp, vp]
         L.ora_uniform.restype = ctypes.c_float
         L.ora_uniform.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
     return _lib
@@ -316,3 +319,16 @@ def prior_reload(udepth: np.ndarray, unormal: np.ndarray, cam, dmin: float, dmax
     c = to_cam(cam)
     lib().ora_prior_reload(_p(udepth), _p(unormal), W, H, ctypes.byref(c), dmin, dmax, _p(prior), _p(mask))
     return prior, mask
+
+
+def cost_grad64(ref, ref_cam, src, src_cam, params, px: int, py: int, theta, with_grad: bool = True):
+    """FP64 differentiable cost of one (pixel, plane, source view) and d cost / d (depth, nx, ny)."""
+    r = np.ascontiguousarray(ref, np.float32)
+    s = np.ascontiguousarray(src, np.float32)
+    th = np.ascontiguousarray(theta, np.float64)
+    g = np.zeros(3, np.float64)
+    rc, sc = to_cam(ref_cam), to_cam(src_cam)
+    prm = to_params(params)
+    c = lib().ora_cost_grad64(_p(r), ctypes.byref(rc), _p(s), ctypes.byref(sc), ctypes.byref(prm), px, py, _p(th),
+                              _p(g) if with_grad else None)
+    return c, g

@@ -13,9 +13,14 @@ import hpm_b200
 from conftest import ROOT, gpu_available
 
 
-def declared_functions() -> list[str]:
+HOST_HEADER = "hpm_host.h"  # declared by libhpm_host.so (image decoding of the command-line driver)
+
+
+def declared_functions(host: bool = False) -> list[str]:
     names = []
     for hdr in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        if (os.path.basename(hdr) == HOST_HEADER) != host:
+            continue
         text = open(hdr).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"^([A-Za-z_][\w \*]*?)\b(hpm_\w+)\s*\(", text, flags=re.M):
@@ -32,6 +37,15 @@ def test_library_exports_every_declared_symbol():
     assert "hpm_run_patchmatch" in names and len(names) >= 15
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
+
+
+def test_host_library_exports_its_symbols():
+    path = os.path.join(os.path.dirname(hpm_b200.LIB_PATH), "libhpm_host.so")
+    assert os.path.exists(path), "build libhpm_host.so first (__graft_entry__.build())"
+    lib = ctypes.CDLL(path)
+    names = declared_functions(host=True)
+    assert "hpm_decode_image" in names
+    assert not [n for n in names if not hasattr(lib, n)]
 
 
 def test_binding_declares_all_symbols():
