@@ -322,7 +322,7 @@ def _measured_hbm():
 
 def _ncu_traffic():
     """dram read+write bytes per k_half_sweep launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "k_half_sweep.md")
+    path = os.path.join(ROOT, "profiles", "k_half_sweep_800x600_s10.md")
     try:
         with open(path) as fh:
             for line in fh:

@@ -44,7 +44,11 @@ EXPORTED_SYMBOLS = (
     "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior", "hpm_set_image", "hpm_prepare_level",
     "hpm_get_level", "hpm_reconstruct", "hpm_get_points", "hpm_get_stream", "hpm_profile_enable",
     "hpm_profile_read", "hpm_measure_fp32_peak", "hpm_eval_costs_noalloc", "hpm_eval_cost_grad", "hpm_gn_refine",
+    "hpm_set_texture_format",
 )
+
+TEX_F32 = 0
+TEX_F16 = 1
 
 PROFILE_TIMING = 1
 PROFILE_COUNT = 2
@@ -189,6 +193,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.hpm_gn_refine.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int,
                                   ctypes.c_int]
     lib.hpm_set_address_mode.argtypes = [vp, ctypes.c_int]
+    lib.hpm_set_texture_format.argtypes = [vp, ctypes.c_int]
     lib.hpm_launch_count.argtypes = [vp]
     lib.hpm_launch_count.restype = ctypes.c_int64
     lib.hpm_synchronize.argtypes = [vp]
@@ -274,6 +279,10 @@ class Context:
         if rc != 0:
             msg = self.lib.hpm_last_error(self.h)
             raise HPMError(f"{what} failed ({rc}): {msg.decode() if msg else ''}")
+
+    def set_texture_format(self, fmt: int) -> None:
+        """TEX_F32 or TEX_F16 texels for the source images bound from now on (hpm_set_texture_format)."""
+        self._check(self.lib.hpm_set_texture_format(self.h, fmt), "hpm_set_texture_format")
 
     def set_address_mode(self, mode: int) -> None:
         self._check(self.lib.hpm_set_address_mode(self.h, mode), "hpm_set_address_mode")

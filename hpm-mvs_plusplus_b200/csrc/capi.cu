@@ -89,6 +89,7 @@ Ctx::~Ctx() {
         cudaEventDestroy(t.stop);
     }
     if (prof_hyp) cudaFree(prof_hyp);
+    if (half_stage) cudaFree(half_stage);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -170,6 +171,15 @@ int hpm_set_address_mode(hpm_ctx* ctx, int mode) {
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     if (mode != 0 && mode != 1) return c->fail(HPM_E_INVALID, "address mode must be 0 (clamp) or 1 (wrap)");
     c->addr_mode = mode;
+    return HPM_OK;
+}
+
+int hpm_set_texture_format(hpm_ctx* ctx, int format) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (format != HPM_TEX_F32 && format != HPM_TEX_F16)
+        return c->fail(HPM_E_INVALID, "texture format must be HPM_TEX_F32 or HPM_TEX_F16");
+    c->tex_format = format;
     return HPM_OK;
 }
 

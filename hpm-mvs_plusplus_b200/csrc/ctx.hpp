@@ -26,7 +26,7 @@ struct ViewState {
     size_t gray_cap = 0;
     cudaArray_t arr = nullptr;
     cudaTextureObject_t tex = 0;
-    int arr_w = 0, arr_h = 0, arr_mode = -1;
+    int arr_w = 0, arr_h = 0, arr_mode = -1, arr_fmt = -1;
     DevMap maps[kNumMaps];
     uint8_t* canny = nullptr;
     size_t canny_cap = 0;
@@ -53,6 +53,8 @@ struct Ctx {
     std::string err;
     std::vector<ViewState> views;
     int addr_mode = 0;
+    int tex_format = 0;  // HPM_TEX_F32 or HPM_TEX_F16: texel type of the source-image textures
+    uint16_t* half_stage = nullptr; size_t half_stage_cap = 0;
     int64_t launches = 0;
 
     // work buffers of one PatchMatch run (sized for the largest reference view)

@@ -3,6 +3,8 @@
 // (HPM.cpp:741-906, 942-984), HPM::RunPatchMatch (HPM.cu:2987-3035) and the
 // result hand-off of ProcessProblem (main.cpp:599-626).
 #include "ctx.hpp"
+
+#include <cuda_fp16.h>
 #include "hpm_geometry.h"
 #include "pm_kernels.cuh"
 #include "aux_kernels.cuh"
@@ -31,17 +33,30 @@ static cudaError_t ensure_buf(T*& p, size_t& cap, size_t n) {
     return e;
 }
 
+__global__ void k_to_half(const float* __restrict__ src, int n, uint16_t* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = __half_as_ushort(__float2half_rn(src[i]));
+}
+
 int Ctx::bind_texture(int view) {
     ViewState& v = views[view];
     cudaError_t e;
-    if (!v.arr || v.arr_w != v.w || v.arr_h != v.h || v.arr_mode != addr_mode) {
+    if (!v.arr || v.arr_w != v.w || v.arr_h != v.h || v.arr_mode != addr_mode || v.arr_fmt != tex_format) {
         if (v.tex) { cudaDestroyTextureObject(v.tex); v.tex = 0; }
-        if (v.arr && (v.arr_w != v.w || v.arr_h != v.h)) { cudaFreeArray(v.arr); v.arr = nullptr; }
+        if (v.arr && (v.arr_w != v.w || v.arr_h != v.h || v.arr_fmt != tex_format)) {
+            cudaFreeArray(v.arr);
+            v.arr = nullptr;
+        }
         if (!v.arr) {
-            cudaChannelFormatDesc fd = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+            // float texels, or half texels: the 0..255 grey levels are exact, the filtered sample is
+            // returned rounded to half precision
+            cudaChannelFormatDesc fd = tex_format == HPM_TEX_F16
+                                           ? cudaCreateChannelDesc(16, 0, 0, 0, cudaChannelFormatKindFloat)
+                                           : cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
             e = cudaMallocArray(&v.arr, &fd, v.w, v.h);
             if (e != cudaSuccess) return cuda_fail(e, "alloc image array");
             v.arr_w = v.w; v.arr_h = v.h;
+            v.arr_fmt = tex_format;
         }
         cudaResourceDesc rd;
         memset(&rd, 0, sizeof(rd));
@@ -59,8 +74,18 @@ int Ctx::bind_texture(int view) {
         if (e != cudaSuccess) return cuda_fail(e, "create texture");
         v.arr_mode = addr_mode;
     }
-    e = cudaMemcpy2DToArrayAsync(v.arr, 0, 0, v.gray, sizeof(float) * v.w, sizeof(float) * v.w, v.h,
-                                 cudaMemcpyDeviceToDevice, stream);
+    if (tex_format == HPM_TEX_F16) {
+        const size_t n = (size_t)v.w * v.h;
+        e = ensure_buf(half_stage, half_stage_cap, n);
+        if (e != cudaSuccess) return cuda_fail(e, "alloc half staging");
+        k_to_half<<<(int)((n + 255) / 256), 256, 0, stream>>>(v.gray, (int)n, half_stage);
+        ++launches;
+        e = cudaMemcpy2DToArrayAsync(v.arr, 0, 0, half_stage, 2 * (size_t)v.w, 2 * (size_t)v.w, v.h,
+                                     cudaMemcpyDeviceToDevice, stream);
+    } else {
+        e = cudaMemcpy2DToArrayAsync(v.arr, 0, 0, v.gray, sizeof(float) * v.w, sizeof(float) * v.w, v.h,
+                                     cudaMemcpyDeviceToDevice, stream);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "copy image to array");
     return HPM_OK;
 }

@@ -238,6 +238,16 @@ int hpm_debug_run_partial(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src,
  * (what HPM.cpp:760-761 requests with unnormalised coordinates). */
 int hpm_set_address_mode(hpm_ctx *ctx, int mode);
 
+/* Texel type of the source-image textures bound from now on (hpm_set_view,
+ * hpm_prepare_level): HPM_TEX_F32 (default, the reference's float textures,
+ * HPM.cpp:750-768) or HPM_TEX_F16, the precision form: half the bytes through
+ * the texture path.  The 8-bit grey levels are stored exactly, but the
+ * filtered sample comes back rounded to half precision (within 1/16 of a grey
+ * level), so F16 results are close to, not equal to, F32 results. */
+#define HPM_TEX_F32 0
+#define HPM_TEX_F16 1
+int hpm_set_texture_format(hpm_ctx *ctx, int format);
+
 /* Kernel launches issued by this context since creation (for accounting). */
 int64_t hpm_launch_count(const hpm_ctx *ctx);
 
