@@ -73,23 +73,65 @@ __global__ void k_support_blocks(const float* __restrict__ costs, const float* _
 
 // Barycentric stepping raster of main.cpp:391-404; labels idx+1, the later
 // triangle wins, so the label is the maximum over the triangles covering a pixel.
-__global__ void k_raster(const hpm_triangle* __restrict__ tris, int n, int width, int* __restrict__ label) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const hpm_triangle T = tris[t];
+// The positions visited are those of the reference's loops,
+//   for (float p = 0; p < 1.0; p += step) for (float q = 0; q < 1.0 - p; q += step),
+// step = 1 / (longest edge): about L^2 / 2 of them for a triangle with longest
+// edge L, from a few for the triangles between neighbouring support points to
+// hundreds of thousands for the ones spanning textureless regions.  Small
+// triangles take one warp each (rows p_k to lanes k mod 32); large ones a block
+// each, with the float sequence 0, step, 2 step, ... (the same for p and q)
+// tabulated once in shared memory.
+__device__ __forceinline__ float raster_step(const hpm_triangle& T) {
     const double d01 = (double)(T.x1 - T.x2) * (T.x1 - T.x2) + (double)(T.y1 - T.y2) * (T.y1 - T.y2);
     const double d02 = (double)(T.x1 - T.x3) * (T.x1 - T.x3) + (double)(T.y1 - T.y3) * (T.y1 - T.y3);
     const double d12 = (double)(T.x2 - T.x3) * (T.x2 - T.x3) + (double)(T.y2 - T.y3) * (T.y2 - T.y3);
     const float L01 = (float)sqrt(d01), L02 = (float)sqrt(d02), L12 = (float)sqrt(d12);
     const float mx = fmaxf(L01, fmaxf(L02, L12));
-    const float step = (float)(1.0 / mx);
-    const int lab = t + 1;
-    for (float p = 0; p < 1.0; p += step)
-        for (float q = 0; q < 1.0 - p; q += step) {
-            const int x = (int)((double)(p * T.x1 + q * T.x2) + (1.0 - p - q) * T.x3);
-            const int y = (int)((double)(p * T.y1 + q * T.y2) + (1.0 - p - q) * T.y3);
-            atomicMax(&label[(size_t)y * width + x], lab);
-        }
+    return (float)(1.0 / mx);
+}
+
+__device__ __forceinline__ void raster_point(const hpm_triangle& T, float p, float q, int width, int lab,
+                                             int* __restrict__ label) {
+    const int x = (int)((double)(p * T.x1 + q * T.x2) + (1.0 - p - q) * T.x3);
+    const int y = (int)((double)(p * T.y1 + q * T.y2) + (1.0 - p - q) * T.y3);
+    atomicMax(&label[(size_t)y * width + x], lab);
+}
+
+__global__ void k_raster(const hpm_triangle* __restrict__ tris, const int32_t* __restrict__ small, int n_small,
+                         int width, int* __restrict__ label) {
+    const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= n_small) return;
+    const int t = small[w];
+    const hpm_triangle T = tris[t];
+    const float step = raster_step(T);
+    int k = 0;
+    for (float p = 0; p < 1.0; p += step, ++k) {
+        if ((k & 31) != lane) continue;
+        for (float q = 0; q < 1.0 - p; q += step) raster_point(T, p, q, width, t + 1, label);
+    }
+}
+
+constexpr int kRasterSeq = 8192;  // longest tabulated step sequence (longest edge up to 8190 px)
+
+__global__ void k_raster_big(const hpm_triangle* __restrict__ tris, const int32_t* __restrict__ big, int width,
+                             int* __restrict__ label) {
+    __shared__ float seq[kRasterSeq];
+    __shared__ int len;
+    const int t = big[blockIdx.x];
+    const hpm_triangle T = tris[t];
+    const float step = raster_step(T);
+    if (threadIdx.x == 0) {
+        int k = 0;
+        for (float v = 0; v < 1.0 && k < kRasterSeq; v += step) seq[k++] = v;
+        len = k;
+    }
+    __syncthreads();
+    for (int k = 0; k < len; ++k) {
+        const float p = seq[k];
+        for (int m = threadIdx.x; m < len && seq[m] < 1.0 - p; m += blockDim.x)
+            raster_point(T, p, seq[m], width, t + 1, label);
+    }
 }
 
 // 3-point plane in the camera frame (HPM.cpp:1099-1167): the unit-normal null
@@ -297,14 +339,33 @@ int Ctx::prior_from_triangles(int view, int distance, const hpm_triangle* tris, 
     const size_t nsmall = (size_t)sup_w * sup_h;
     // triangles (24 bytes each) then the float4 planes at a 256-byte aligned offset
     const size_t planes_off = ((size_t)std::max(na, 1) * sizeof(hpm_triangle) + 255) & ~size_t(255);
-    cudaError_t e = ensure_p(prior_tris, prior_tris_cap, planes_off + (size_t)std::max(na, 1) * 16);
+    const size_t lists_off = planes_off + (((size_t)std::max(na, 1) * 16 + 255) & ~size_t(255));
+    // raster work lists: triangles whose longest edge is at most kSmallEdge go one per warp,
+    // the others one per block (same float step as the kernel: double lengths, float max)
+    const float kSmallEdge = 64.0f;
+    std::vector<int32_t> lists((size_t)std::max(na, 1));
+    int n_small = 0, n_big = 0;
+    for (int t = 0; t < na; ++t) {
+        const hpm_triangle& T = acc[t];
+        const double d01 = (double)(T.x1 - T.x2) * (T.x1 - T.x2) + (double)(T.y1 - T.y2) * (T.y1 - T.y2);
+        const double d02 = (double)(T.x1 - T.x3) * (T.x1 - T.x3) + (double)(T.y1 - T.y3) * (T.y1 - T.y3);
+        const double d12 = (double)(T.x2 - T.x3) * (T.x2 - T.x3) + (double)(T.y2 - T.y3) * (T.y2 - T.y3);
+        const float mx = std::max((float)std::sqrt(d01), std::max((float)std::sqrt(d02), (float)std::sqrt(d12)));
+        // (edges beyond the block kernel's table stay on the warp path, slow but exact)
+        if (mx <= kSmallEdge || mx > (float)(kRasterSeq - 8)) lists[n_small++] = t;
+        else lists[na - 1 - n_big++] = t;
+    }
+    cudaError_t e = ensure_p(prior_tris, prior_tris_cap, lists_off + (size_t)std::max(na, 1) * 4);
     if (e != cudaSuccess) return cuda_fail(e, "alloc triangles");
     hpm_triangle* d_tris = reinterpret_cast<hpm_triangle*>(prior_tris);
     float4* d_planes = reinterpret_cast<float4*>(prior_tris + planes_off);
     e = ensure_p(prior_label, prior_label_cap, nsmall);
     if (e != cudaSuccess) return cuda_fail(e, "alloc labels");
+    int32_t* d_lists = reinterpret_cast<int32_t*>(prior_tris + lists_off);
     if (na > 0) {
         e = cudaMemcpyAsync(d_tris, acc.data(), sizeof(hpm_triangle) * na, cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_lists, lists.data(), sizeof(int32_t) * na, cudaMemcpyHostToDevice, stream);
         if (e != cudaSuccess) return cuda_fail(e, "upload triangles");
     }
     cudaMemsetAsync(prior_label, 0, sizeof(int) * nsmall, stream);
@@ -314,8 +375,15 @@ int Ctx::prior_from_triangles(int view, int distance, const hpm_triangle* tris, 
     const hpm_camera& cam = v.cam;
     const float dmin = cam.depth_min * 0.6f, dmax = cam.depth_max * 1.2f;  // params range (HPM.cpp:685-686)
     if (na > 0) {
-        k_raster<<<(na + 63) / 64, 64, 0, stream>>>(d_tris, na, sup_w, prior_label);
-        ++launches;
+        if (n_small > 0) {
+            k_raster<<<(int)(((size_t)n_small * 32 + 255) / 256), 256, 0, stream>>>(d_tris, d_lists, n_small, sup_w,
+                                                                                    prior_label);
+            ++launches;
+        }
+        if (n_big > 0) {
+            k_raster_big<<<n_big, 256, 0, stream>>>(d_tris, d_lists + (na - n_big), sup_w, prior_label);
+            ++launches;
+        }
     }
     if (distance == 0) {
         if (na > 0) {
