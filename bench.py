@@ -85,6 +85,8 @@ def parse_args():
     ap.add_argument("--scale", type=int, default=1, help="--initial-image-scale")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--chosen-form", action=argparse.BooleanOptionalAction, default=True,
+                    help="also time the precision form (F16 source textures)")
     return ap.parse_args()
 
 
@@ -309,7 +311,35 @@ def run_ours(args, scene, rank, world, local_rank):
         "clocks": clocks,
         "roofline": roofline,
     }
+    if args.chosen_form:
+        result["chosen_form"] = chosen_form(args, ctx, step, n_views, world, device)
     return result, ctx, images
+
+
+def chosen_form(args, ctx, step, n_views, world, device):
+    """The same steps with half-precision source textures (hpm_set_texture_format), the precision
+    form: 8-bit grey levels stored exactly, filtered samples rounded to half precision."""
+    import torch
+    hb = _import_pkg()
+    ctx.set_texture_format(hb.TEX_F16)
+    for _ in range(max(1, min(args.warmup, 2))):
+        step()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    evs = [step()[0] for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    ctx.set_texture_format(hb.TEX_F32)
+    dev_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
+    e2e_ms = sum(e[0].elapsed_time(e[3]) for e in evs)
+    t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total_views = n_views * args.steps * world
+    return {"form": "F16 source textures (within 1/16 grey level of F32; same accuracy against the rendered "
+                    "ground truth, tests/test_gpu_texf16.py)",
+            "value": total_views / (float(t[0]) / 1e3), "e2e": total_views / (float(t[1]) / 1e3),
+            "unit": UNIT, "ms_per_step": float(t[0]) / args.steps}
 
 
 def _measured_hbm():
