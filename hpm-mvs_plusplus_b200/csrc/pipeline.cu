@@ -17,17 +17,6 @@ namespace hpm {
 
 int delaunay_triangulate(const int32_t* xy, int n, int width, int height, std::vector<hpm_triangle>& out);
 
-namespace {
-
-uint64_t mix_seed(uint64_t base, uint64_t a, uint64_t b) {
-    uint64_t z = base ^ (a * 0x9E3779B97F4A7C15ULL) ^ (b * 0xBF58476D1CE4E5B9ULL);
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-    return z ^ (z >> 31);
-}
-
-}  // namespace
-
 int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off, const int32_t* src_ids,
                      const hpm_recon_options* opt, int64_t* n_points_out) {
     cudaSetDevice(device);
@@ -76,7 +65,7 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
         p.scaled_rows = 0;
         p.mode = mode;
         return run_patchmatch(i, src_ids + src_off[i], p.num_images - 1, &p, texture_level,
-                              mix_seed(opt->seed, (uint64_t)pass, (uint64_t)i));
+                              hpm_run_seed(opt->seed, (uint64_t)pass, (uint64_t)i));
     };
     auto confidence = [&](int depth_kind) -> int {
         return consistency_scan(0, n_views, src_off, src_ids, depth_kind, nullptr, nullptr, 0, nullptr, nullptr);

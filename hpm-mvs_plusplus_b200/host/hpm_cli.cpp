@@ -12,7 +12,10 @@
 // --mask fuses with the sky masks masks/%08d.jpg (RunFusion_Sky_Strict);
 // the environment variable HPM_SEED (decimal) fixes the random streams;
 // --fusion-only skips the reconstruction and fuses the existing
-// depths_geom.dmb / normals.dmb.
+// depths_geom.dmb / normals.dmb; --per-problem runs the reference's main loop
+// problem by problem through the HPM class, with .dmb files between the
+// stages (same results as the default resident schedule).  HPM_LEVEL_MAX_SIDE
+// (default 1000) is the pyramid bound of main.cpp:205, for small test inputs.
 #include <sys/stat.h>
 
 #include <chrono>
@@ -27,9 +30,15 @@
 
 #include "formats.hpp"
 #include "hpm_capi.h"
+#include "hpm_class.hpp"
 #include "hpm_host.h"
 
 using namespace hpm_host;
+
+namespace hpm_host {
+int64_t run_per_problem(const std::string& folder, const std::vector<Problem>& pairs, int scale, uint64_t seed,
+                        int level_max_side, const std::vector<int32_t>& src_off, const std::vector<int32_t>& src_ids);
+}
 
 namespace {
 
@@ -89,7 +98,7 @@ int main(int argc, char** argv) {
         return -1;
     }
     const std::string folder = argv[1];
-    bool mask_flag = false, fuse_only = false, show_medium = false;
+    bool mask_flag = false, fuse_only = false, show_medium = false, per_problem = false;
     int scale = 4;
     try {
         for (int a = 2; a < argc;) {
@@ -97,6 +106,7 @@ int main(int argc, char** argv) {
             if (opt == "--mask") mask_flag = true;
             else if (opt == "--fusion-only" || opt == "--fuse") fuse_only = true;
             else if (opt == "--show-medium-result") show_medium = true;
+            else if (opt == "--per-problem") per_problem = true;
             else if (opt == "--initial-image-scale" && a < argc) {
                 const std::string v(argv[a++]);
                 size_t parsed = 0;
@@ -131,7 +141,8 @@ int main(int argc, char** argv) {
             src_off.push_back((int32_t)src_ids.size());
         }
         std::cout << "There are " << n << " problems needed to be processed!" << std::endl;
-        check(ctx, hpm_create(0, &ctx), "hpm_create");
+        if (per_problem) ctx = HPM::context();
+        else check(ctx, hpm_create(0, &ctx), "hpm_create");
         std::vector<hpm_camera> cams(n);
         std::vector<Image> images(n);
         for (int i = 0; i < n; ++i) {
@@ -141,7 +152,8 @@ int main(int argc, char** argv) {
                 throw std::runtime_error("cannot read " + folder + "/cams/" + id8(i) + "_cam.txt");
             cams[i].width = images[i].w;
             cams[i].height = images[i].h;
-            check(ctx, hpm_set_image(ctx, i, images[i].bgr.data(), images[i].w, images[i].h), "hpm_set_image");
+            if (!per_problem)
+                check(ctx, hpm_set_image(ctx, i, images[i].bgr.data(), images[i].w, images[i].h), "hpm_set_image");
         }
         const std::string out_folder = folder + "/HPM_MVS_plusplus";
         mkdir(out_folder.c_str(), 0755);
@@ -171,10 +183,22 @@ int main(int argc, char** argv) {
             // the reference seeds from the clock (HPM.cu:579); HPM_SEED fixes the streams for reproducible runs
             opt.seed = (uint64_t)std::chrono::steady_clock::now().time_since_epoch().count();
             if (const char* env = std::getenv("HPM_SEED")) opt.seed = std::strtoull(env, nullptr, 10);
-            int64_t unused = 0;
-            check(ctx, hpm_reconstruct(ctx, n, cams.data(), src_off.data(), src_ids.data(), &opt, &unused),
-                  "hpm_reconstruct");
-            for (int i = 0; i < n; ++i) {
+            if (const char* env = std::getenv("HPM_LEVEL_MAX_SIDE")) opt.level_max_side = std::atoi(env);
+            if (per_problem) {
+                run_per_problem(folder, problems, scale, opt.seed, opt.level_max_side, src_off, src_ids);
+                if (!show_medium)  // RemoveIntermediateResults (main.cpp:1111-1141)
+                    for (int i = 0; i < n; ++i) {
+                        const std::string dir = out_folder + "/2333_" + id8(i);
+                        std::remove((dir + "/costs.dmb").c_str());
+                        std::remove((dir + "/confidence.dmb").c_str());
+                        for (int k = 0; k < 8; ++k) std::remove((dir + "/texture" + std::to_string(k) + ".dmb").c_str());
+                    }
+            } else {
+                int64_t unused = 0;
+                check(ctx, hpm_reconstruct(ctx, n, cams.data(), src_off.data(), src_ids.data(), &opt, &unused),
+                      "hpm_reconstruct");
+            }
+            for (int i = 0; i < n && !per_problem; ++i) {
                 const std::string dir = out_folder + "/2333_" + id8(i);
                 mkdir(dir.c_str(), 0755);
                 int w, h;
@@ -225,10 +249,12 @@ int main(int argc, char** argv) {
                   << " with unit normals to " << out_folder << "/fused.ply" << std::endl;
     } catch (const std::exception& e) {
         std::cerr << e.what() << std::endl;
-        if (ctx) hpm_destroy(ctx);
+        if (per_problem) HPM::release_context();
+        else if (ctx) hpm_destroy(ctx);
         return EXIT_FAILURE;
     }
-    hpm_destroy(ctx);
+    if (per_problem) HPM::release_context();
+    else hpm_destroy(ctx);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     std::cout << "Total execution time: " << secs << " seconds" << std::endl;
     return 0;

@@ -67,6 +67,18 @@ typedef struct hpm_triangle {
 #define HPM_MAX_SRC 31      /* 32-bit view masks and cost_vector[32] (HPM.cu:453) cap S at 31 */
 #define HPM_MAX_VIEWS 256   /* MAX_IMAGES (main.h:36) */
 
+/* Seed of the PatchMatch run of `view` in pass `pass` of a reconstruction
+ * keyed by `base` (a splitmix64-style mix): hpm_reconstruct uses it with
+ * passes counted from 1 in schedule order, so a caller that drives the same
+ * schedule run by run draws the same random streams. */
+static inline uint64_t hpm_run_seed(uint64_t base, uint64_t pass, uint64_t view)
+{
+    uint64_t z = base ^ (pass * 0x9E3779B97F4A7C15ULL) ^ (view * 0xBF58476D1CE4E5B9ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
 #ifdef __cplusplus
 }
 #endif

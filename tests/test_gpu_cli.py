@@ -110,3 +110,29 @@ def test_cli_rejects_bad_arguments(tmp_path):
     assert r.returncode != 0 and "positive integer" in r.stderr
     r = subprocess.run([CLI, str(tmp_path)], capture_output=True, text=True)
     assert r.returncode != 0 and "pair.txt" in r.stderr
+
+
+def test_per_problem_mode_matches_resident_schedule(tmp_path):
+    """--per-problem: the reference's main loop through the HPM class with .dmb files between stages,
+    two pyramid levels (HPM_LEVEL_MAX_SIDE=100 on 160x120 views), against the default resident run."""
+    import shutil
+    from hpm_b200 import synth
+
+    sc = synth.make_scene(n_views=5, width=160, height=120, seed=2, n_src=4)
+    a, b = str(tmp_path / "resident"), str(tmp_path / "per_problem")
+    synth.write_dense_folder(sc, a)
+    shutil.copytree(a, b)
+    env = dict(os.environ, HPM_SEED="13", HPM_LEVEL_MAX_SIDE="100")
+    for folder, extra in ((a, []), (b, ["--per-problem"])):
+        r = subprocess.run([CLI, folder, "--initial-image-scale", "1", *extra], env=env, capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    for i in range(5):
+        for name in ("depths.dmb", "depths_geom.dmb", "normals.dmb"):
+            x = read_dmb(os.path.join(a, "HPM_MVS_plusplus", f"2333_{i:08d}", name))
+            y = read_dmb(os.path.join(b, "HPM_MVS_plusplus", f"2333_{i:08d}", name))
+            assert x.shape == y.shape and same(x, y), (i, name)
+        assert not os.path.exists(os.path.join(b, "HPM_MVS_plusplus", f"2333_{i:08d}", "costs.dmb"))
+    na, pa = read_ply(os.path.join(a, "HPM_MVS_plusplus", "HPM_MVS_plusplus.ply"))
+    nb, pb = read_ply(os.path.join(b, "HPM_MVS_plusplus", "HPM_MVS_plusplus.ply"))
+    assert na == nb and np.array_equal(pa["f"], pb["f"])
