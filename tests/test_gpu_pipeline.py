@@ -82,3 +82,28 @@ def test_reconstruct_matches_oracle_pipeline(ctx, level_max_side):
     assert n_pts == n_ref
     got = ctx.get_points()
     assert np.array_equal(got, pts.reshape(got.shape), equal_nan=True)
+
+
+def test_c1_configuration_matches_oracle_pipeline(ctx):
+    """The reference's small configuration: 5 views of 1280x960 on a 30-degree arc, 4 sources each,
+    --initial-image-scale 4 (320x240 working size, one level), the whole schedule with fusion."""
+    import pipeline as op
+    from hpm_b200 import synth
+
+    sc = synth.make_scene(n_views=5, width=1280, height=960, layout="arc", n_src=4, seed=17)
+    cams = scene_cams(sc)
+    srcs = [[j for j, _ in p] for p in sc.pairs]
+    for i, v in enumerate(sc.views):
+        ctx.set_image(i, v.image)
+    n_pts = ctx.reconstruct(cams, srcs, initial_image_scale=4, seed=23, fuse=True)
+    P = op.OraclePipeline([v.image for v in sc.views], cams, srcs, initial_image_scale=4, seed=23,
+                          triangulate=hpm_b200.delaunay)
+    pts, n_ref = P.reconstruct(fuse=True)
+    for i, v in enumerate(P.views):
+        for kind, key in ((hpm_b200.MAP_DEPTH_GEOM, "depth_geom"), (hpm_b200.MAP_NORMAL, "normal")):
+            g = ctx.get_map(i, kind)
+            o = np.ascontiguousarray(v.maps[key], np.float32)
+            assert g.shape == o.shape == ((240, 320, 3) if key == "normal" else (240, 320))
+            eq = (g.view(np.uint32) == o.view(np.uint32)) | (np.isnan(g) & np.isnan(o))
+            assert eq.all(), (i, key, float(eq.mean()))
+    assert n_pts == n_ref
