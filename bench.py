@@ -266,10 +266,7 @@ def run_ours(args, scene, rank, world, local_rank):
         torch.distributed.barrier()
     dev_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
     e2e_ms = sum(e[0].elapsed_time(e[3]) for e in evs)
-    t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=device)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    dev_ms, e2e_ms = float(t[0]), float(t[1])
+    dev_ms, e2e_ms = max_over_ranks([dev_ms, e2e_ms], world, device)
     total_views = n_views * args.steps * world
     value = total_views / (dev_ms / 1e3)
     e2e = total_views / (e2e_ms / 1e3)
@@ -332,14 +329,22 @@ def chosen_form(args, ctx, step, n_views, world, device):
     ctx.set_texture_format(hb.TEX_F32)
     dev_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
     e2e_ms = sum(e[0].elapsed_time(e[3]) for e in evs)
-    t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device=device)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    t = max_over_ranks([dev_ms, e2e_ms], world, device)
     total_views = n_views * args.steps * world
     return {"form": "F16 source textures (within 1/16 grey level of F32; same accuracy against the rendered "
                     "ground truth, tests/test_gpu_texf16.py)",
             "value": total_views / (float(t[0]) / 1e3), "e2e": total_views / (float(t[1]) / 1e3),
             "unit": UNIT, "ms_per_step": float(t[0]) / args.steps}
+
+
+def max_over_ranks(values, world: int, device):
+    """Element-wise maximum of per-rank timings over the process group (the job ends with its slowest replica)."""
+    import torch
+    if world <= 1:
+        return [float(v) for v in values]
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t]
 
 
 def _measured_hbm():

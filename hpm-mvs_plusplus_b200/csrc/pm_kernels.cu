@@ -887,7 +887,11 @@ static cudaError_t sweep_impl(const RunArgs& a, int color, int iter, cudaStream_
     auto k = k_half_sweep<NS, BLK, MAND, CNT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     if (e != cudaSuccess) return e;
-    dim3 block(32, BLK / 32), grid((a.W + 31) / 32, (a.cover_pairs + BLK / 32 - 1) / (BLK / 32));
+#ifndef HPM_SWEEP_BX
+#define HPM_SWEEP_BX 32
+#endif
+    constexpr int BX = HPM_SWEEP_BX < BLK ? HPM_SWEEP_BX : BLK;
+    dim3 block(BX, BLK / BX), grid((a.W + BX - 1) / BX, (a.cover_pairs + BLK / BX - 1) / (BLK / BX));
     k<<<grid, block, shm, st>>>(a, color, iter);
     return cudaGetLastError();
 }
