@@ -49,6 +49,7 @@ EXPORTED_SYMBOLS = (
 
 TEX_F32 = 0
 TEX_F16 = 1
+TEX_U8 = 2
 
 PROFILE_TIMING = 1
 PROFILE_COUNT = 2

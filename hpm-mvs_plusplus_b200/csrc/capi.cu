@@ -177,8 +177,8 @@ int hpm_set_address_mode(hpm_ctx* ctx, int mode) {
 int hpm_set_texture_format(hpm_ctx* ctx, int format) {
     if (!ctx) return HPM_E_INVALID;
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
-    if (format != HPM_TEX_F32 && format != HPM_TEX_F16)
-        return c->fail(HPM_E_INVALID, "texture format must be HPM_TEX_F32 or HPM_TEX_F16");
+    if (format != HPM_TEX_F32 && format != HPM_TEX_F16 && format != HPM_TEX_U8)
+        return c->fail(HPM_E_INVALID, "texture format must be HPM_TEX_F32, HPM_TEX_F16 or HPM_TEX_U8");
     c->tex_format = format;
     return HPM_OK;
 }

@@ -142,7 +142,7 @@ __device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int 
     }
     s_s *= P.rs.inv_w; s_ss *= P.rs.inv_w; s_rs *= P.rs.inv_w;
     const float var_s = s_ss - s_s * s_s;
-    if (var_s < 1e-5f) return cost_max;
+    if (var_s < a.var_s_min) return cost_max;
     const float cov = s_rs - P.rs.mean * s_s;
     const float vrs = sqrtf(P.rs.var * var_s);
     return fmaxf(0.0f, fminf(cost_max, 1.0f - cov / vrs));

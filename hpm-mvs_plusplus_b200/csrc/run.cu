@@ -38,6 +38,11 @@ __global__ void k_to_half(const float* __restrict__ src, int n, uint16_t* __rest
     if (i < n) dst[i] = __half_as_ushort(__float2half_rn(src[i]));
 }
 
+__global__ void k_to_u8(const float* __restrict__ src, int n, uint8_t* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = (uint8_t)fminf(255.0f, fmaxf(0.0f, rintf(src[i])));
+}
+
 int Ctx::bind_texture(int view) {
     ViewState& v = views[view];
     cudaError_t e;
@@ -52,7 +57,9 @@ int Ctx::bind_texture(int view) {
             // returned rounded to half precision
             cudaChannelFormatDesc fd = tex_format == HPM_TEX_F16
                                            ? cudaCreateChannelDesc(16, 0, 0, 0, cudaChannelFormatKindFloat)
-                                           : cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
+                                           : (tex_format == HPM_TEX_U8
+                                                  ? cudaCreateChannelDesc(8, 0, 0, 0, cudaChannelFormatKindUnsigned)
+                                                  : cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat));
             e = cudaMallocArray(&v.arr, &fd, v.w, v.h);
             if (e != cudaSuccess) return cuda_fail(e, "alloc image array");
             v.arr_w = v.w; v.arr_h = v.h;
@@ -68,7 +75,7 @@ int Ctx::bind_texture(int view) {
         td.addressMode[0] = am;
         td.addressMode[1] = am;
         td.filterMode = cudaFilterModeLinear;
-        td.readMode = cudaReadModeElementType;
+        td.readMode = tex_format == HPM_TEX_U8 ? cudaReadModeNormalizedFloat : cudaReadModeElementType;
         td.normalizedCoords = 0;
         e = cudaCreateTextureObject(&v.tex, &rd, &td, nullptr);
         if (e != cudaSuccess) return cuda_fail(e, "create texture");
@@ -82,6 +89,15 @@ int Ctx::bind_texture(int view) {
         ++launches;
         e = cudaMemcpy2DToArrayAsync(v.arr, 0, 0, half_stage, 2 * (size_t)v.w, 2 * (size_t)v.w, v.h,
                                      cudaMemcpyDeviceToDevice, stream);
+    } else if (tex_format == HPM_TEX_U8) {
+        const size_t n = (size_t)v.w * v.h;
+        e = ensure_buf(half_stage, half_stage_cap, n);  // n bytes fit in the n half words
+        if (e != cudaSuccess) return cuda_fail(e, "alloc byte staging");
+        uint8_t* bytes = reinterpret_cast<uint8_t*>(half_stage);
+        k_to_u8<<<(int)((n + 255) / 256), 256, 0, stream>>>(v.gray, (int)n, bytes);
+        ++launches;
+        e = cudaMemcpy2DToArrayAsync(v.arr, 0, 0, bytes, (size_t)v.w, (size_t)v.w, v.h, cudaMemcpyDeviceToDevice,
+                                     stream);
     } else {
         e = cudaMemcpy2DToArrayAsync(v.arr, 0, 0, v.gray, sizeof(float) * v.w, sizeof(float) * v.w, v.h,
                                      cudaMemcpyDeviceToDevice, stream);
@@ -110,6 +126,8 @@ int Ctx::fill_run_args(int ref, const int32_t* srcs, int n_src, const hpm_params
         hpm_view_basis(&rv.cam, &views[s].cam, a.basis[j + 1].A, a.basis[j + 1].b);
     }
     hpm_ref_kinv(&rv.cam, a.kinv);
+    // 8-bit textures return grey / 255; the NCC is scale-free, only the flat-source test scales
+    a.var_s_min = tex_format == HPM_TEX_U8 ? 1e-5f / (255.0f * 255.0f) : 1e-5f;
     a.ref_img = rv.gray;
     a.prm = *params;
     a.S = n_src;

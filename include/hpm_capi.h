@@ -246,6 +246,7 @@ int hpm_set_address_mode(hpm_ctx *ctx, int mode);
  * level), so F16 results are close to, not equal to, F32 results. */
 #define HPM_TEX_F32 0
 #define HPM_TEX_F16 1
+#define HPM_TEX_U8 2  /* 8-bit texels read as grey/255; the NCC is scale-free, its flat-source test is rescaled */
 int hpm_set_texture_format(hpm_ctx *ctx, int format);
 
 /* Kernel launches issued by this context since creation (for accounting). */

@@ -1,4 +1,9 @@
-"""Half-precision source textures (hpm_set_texture_format(HPM_TEX_F16)) on the B200.
+"""Half-precision and 8-bit source textures (hpm_set_texture_format) on the B200.
+
+HPM_TEX_U8 stores the grey levels exactly in one byte and reads them back as
+grey / 255; the NCC is scale-free, so only its flat-source threshold is
+rescaled.  Its per-hypothesis cost error against the FP64 exact-bilinear cost
+matches the float-texel path's, and so does the reconstruction accuracy.
 
 The grey levels of 8-bit images (integers 0..255) are stored exactly in half
 precision, but the texture unit returns a filtered half texel rounded to half
@@ -59,7 +64,7 @@ def test_cost_error_against_fp64(small_scene):
     planes = np.asarray(planes, np.float32)
     errs = {}
     with hpm_b200.Context(0) as ctx:
-        for fmt in (hpm_b200.TEX_F32, hpm_b200.TEX_F16):
+        for fmt in (hpm_b200.TEX_F32, hpm_b200.TEX_F16, hpm_b200.TEX_U8):
             ctx.set_texture_format(fmt)
             for i, (g, c) in enumerate(zip(grays, cams)):
                 ctx.set_view(i, g, c)
@@ -72,10 +77,12 @@ def test_cost_error_against_fp64(small_scene):
                     if 0 < c64 < 2 and 0 < got[k, j] < 2:
                         e.append(abs(got[k, j] - c64))
             errs[fmt] = np.asarray(e)
-    p32, p16 = (np.quantile(errs[f], 0.99) for f in (hpm_b200.TEX_F32, hpm_b200.TEX_F16))
-    print(f"cost error vs FP64 exact bilinear, p99: f32 texels {p32:.2e}, f16 texels {p16:.2e}; "
-          f"median: {np.median(errs[hpm_b200.TEX_F32]):.2e}, {np.median(errs[hpm_b200.TEX_F16]):.2e}")
+    p32, p16, p8 = (np.quantile(errs[f], 0.99) for f in (hpm_b200.TEX_F32, hpm_b200.TEX_F16, hpm_b200.TEX_U8))
+    print(f"cost error vs FP64 exact bilinear, p99: f32 texels {p32:.2e}, f16 texels {p16:.2e}, u8 texels {p8:.2e}; "
+          f"median: {np.median(errs[hpm_b200.TEX_F32]):.2e}, {np.median(errs[hpm_b200.TEX_F16]):.2e}, "
+          f"{np.median(errs[hpm_b200.TEX_U8]):.2e}")
     assert p16 <= 1.5 * p32 + 2e-3
+    assert p8 <= 1.5 * p32 + 2e-3
 
 
 def test_reconstruction_accuracy_with_half_texels():
@@ -85,7 +92,7 @@ def test_reconstruction_accuracy_with_half_texels():
     cams = scene_cams(sc)
     srcs = [[j for j, _ in p] for p in sc.pairs]
     acc = {}
-    for fmt in (hpm_b200.TEX_F32, hpm_b200.TEX_F16):
+    for fmt in (hpm_b200.TEX_F32, hpm_b200.TEX_F16, hpm_b200.TEX_U8):
         with hpm_b200.Context(0) as ctx:
             ctx.set_texture_format(fmt)
             for i, v in enumerate(sc.views):
@@ -98,5 +105,6 @@ def test_reconstruction_accuracy_with_half_texels():
                 a.append(float((np.abs(d - v.depth)[ok] / v.depth[ok] < 0.01).mean()))
             acc[fmt] = np.mean(a)
     print(f"pixels within 1 % of the true depth: f32 texels {acc[hpm_b200.TEX_F32]:.3f}, "
-          f"f16 texels {acc[hpm_b200.TEX_F16]:.3f}")
+          f"f16 texels {acc[hpm_b200.TEX_F16]:.3f}, u8 texels {acc[hpm_b200.TEX_U8]:.3f}")
     assert acc[hpm_b200.TEX_F16] >= acc[hpm_b200.TEX_F32] - 0.02
+    assert acc[hpm_b200.TEX_U8] >= acc[hpm_b200.TEX_F32] - 0.02
