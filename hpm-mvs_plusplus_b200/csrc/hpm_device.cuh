@@ -124,47 +124,26 @@ __device__ __forceinline__ float4 perturbed_normal(const hpm_camera& c, int px, 
     return np;
 }
 
-__device__ __forceinline__ float3 point_world(float x, float y, float depth, const hpm_camera& c) {
-    const float X0 = depth * (x - c.K[2]) / c.K[0];
-    const float X1 = depth * (y - c.K[5]) / c.K[4];
-    const float X2 = depth;
-    const float T0 = c.R[0] * X0 + c.R[3] * X1 + c.R[6] * X2;
-    const float T1 = c.R[1] * X0 + c.R[4] * X1 + c.R[7] * X2;
-    const float T2 = c.R[2] * X0 + c.R[5] * X1 + c.R[8] * X2;
-    const float C0 = -(c.R[0] * c.t[0] + c.R[3] * c.t[1] + c.R[6] * c.t[2]);
-    const float C1 = -(c.R[1] * c.t[0] + c.R[4] * c.t[1] + c.R[7] * c.t[2]);
-    const float C2 = -(c.R[2] * c.t[0] + c.R[5] * c.t[1] + c.R[8] * c.t[2]);
-    return make_float3(T0 + C0, T1 + C1, T2 + C2);
-}
-
-__device__ __forceinline__ float2 project_point(float3 X, const hpm_camera& c, float& depth) {
-    const float T0 = c.R[0] * X.x + c.R[1] * X.y + c.R[2] * X.z + c.t[0];
-    const float T1 = c.R[3] * X.x + c.R[4] * X.y + c.R[5] * X.z + c.t[1];
-    const float T2 = c.R[6] * X.x + c.R[7] * X.y + c.R[8] * X.z + c.t[2];
-    depth = c.K[6] * T0 + c.K[7] * T1 + c.K[8] * T2;
-    return make_float2((c.K[0] * T0 + c.K[1] * T1 + c.K[2] * T2) / depth,
-                       (c.K[3] * T0 + c.K[4] * T1 + c.K[5] * T2) / depth);
-}
-
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// ComputeGeomConsistencyCost (HPM.cu:539-564).  The source depth is sampled at
-// texel centres ((int)x + 0.5), i.e. a clamped point fetch.
-__device__ __forceinline__ float geom_cost(const float* __restrict__ sdepth, int sw, int sh, const hpm_camera& rc,
-                                           const hpm_camera& sc, float4 pl, int px, int py) {
+// ComputeGeomConsistencyCost (HPM.cu:539-564): the pixel's 3D point at the
+// hypothesis depth carried into source j, the source depth read there (a
+// clamped point fetch at (int)x, (int)y) and carried back; the cost is the
+// reprojection distance, at most 3.  The two transfers use the per-view bases
+// of hpm_view_transfer (include/hpm_geometry.h).
+__device__ __forceinline__ float geom_cost(const float* __restrict__ sdepth, int sw, int sh, const float* Gf,
+                                           const float* gf, const float* Gb, const float* gb, float depth, int px,
+                                           int py) {
     const float max_cost = 3.0f;
-    const float depth = depth_from_plane(rc, pl, px, py);
-    const float3 fwd = point_world((float)px, (float)py, depth, rc);
-    float sd;
-    const float2 spt = project_point(fwd, sc, sd);
-    const int ix = clampi(__float2int_rz(spt.x), 0, sw - 1);
-    const int iy = clampi(__float2int_rz(spt.y), 0, sh - 1);
+    float sx, sy;
+    hpm_transfer(Gf, gf, (float)px, (float)py, depth, &sx, &sy);
+    const int ix = clampi(__float2int_rz(sx), 0, sw - 1);
+    const int iy = clampi(__float2int_rz(sy), 0, sh - 1);
     const float d = __ldg(sdepth + (size_t)iy * sw + ix);
     if (d == 0.0f) return max_cost;
-    const float3 sX = point_world(spt.x, spt.y, d, sc);
-    float rd;
-    const float2 bwd = project_point(sX, rc, rd);
-    const float dx = px - bwd.x, dy = py - bwd.y;
+    float bx, by;
+    hpm_transfer(Gb, gb, sx, sy, d, &bx, &by);
+    const float dx = px - bx, dy = py - by;
     return fminf(max_cost, sqrtf(dx * dx + dy * dy));
 }
 

@@ -486,15 +486,16 @@ __device__ __forceinline__ Selection view_selection(const RunArgs& a, int px, in
     for (int d = 0; d < 8; ++d) {
         float fc = 0.0f;
         const bool valid = flags & (1u << d);
-        float4 pl = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (geom && valid) pl = a.planes[s.pos(d)];
+        float depth = 0.0f;
+        if (geom && valid) depth = depth_from_plane(a.cams[0], a.planes[s.pos(d)], px, py);
         for (int j = 0; j < S; ++j) {
             const float w = s.vw(j);
             if (w > 0) {
                 if (geom) {
                     if (valid)
                         fc += w * (s.ca(d, j) + 0.2f * geom_cost(a.depth_src[j + 1], a.dsw[j + 1], a.dsh[j + 1],
-                                                                   a.cams[0], a.cams[j + 1], pl, px, py));
+                                                                   a.fwd[j + 1].A, a.fwd[j + 1].b, a.bwd[j + 1].A,
+                                                                   a.bwd[j + 1].b, depth, px, py));
                     else
                         fc += w * (s.ca(d, j) + 0.1f * 3.0f);
                 } else {
@@ -513,14 +514,16 @@ template <int NS, int BLK, bool CNT>
 __device__ __forceinline__ float selected_cost(const RunArgs& a, int px, int py, float4 pl, uint32_t selmask,
                                                float weight_norm, const Scratch<NS, BLK, CNT>& s) {
     const bool geom = a.prm.mode & HPM_MODE_GEOM;
+    const float depth = geom ? depth_from_plane(a.cams[0], pl, px, py) : 0.0f;
     float c = 0.0f;
 #pragma unroll 1
     for (int j = 0; j < a.S; ++j) {
         if (!((selmask >> j) & 1u)) continue;
         const float w = s.vw(j);
         const float n = s.ca(8, j);
-        if (geom) c += w * (n + 0.2f * geom_cost(a.depth_src[j + 1], a.dsw[j + 1], a.dsh[j + 1], a.cams[0],
-                                                  a.cams[j + 1], pl, px, py));
+        if (geom) c += w * (n + 0.2f * geom_cost(a.depth_src[j + 1], a.dsw[j + 1], a.dsh[j + 1], a.fwd[j + 1].A,
+                                                  a.fwd[j + 1].b, a.bwd[j + 1].A, a.bwd[j + 1].b, depth, px,
+                                                  py));
         else c += w * n;
     }
     return c / weight_norm;

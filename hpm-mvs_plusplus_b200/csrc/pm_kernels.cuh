@@ -19,7 +19,8 @@ struct ViewBasis {
 // as a __grid_constant__ kernel parameter (about 6 KB).
 struct RunArgs {
     hpm_camera cams[32];            // 0 = reference
-    ViewBasis basis[32];            // homography basis of source j+1 w.r.t. the reference
+    ViewBasis basis[32];
+    ViewBasis fwd[32], bwd[32];     // geometric cost: point transfer reference -> source j+1 and back            // homography basis of source j+1 w.r.t. the reference
     float kinv[4];                  // 1/fx, 1/fy, cx/fx, cy/fy of the reference camera
     float var_s_min;                // flat-source threshold: 1e-5 (HPM.cu:434) in the textures' grey units
     cudaTextureObject_t tex[32];    // linear-filtered source images (index j+1)
@@ -46,7 +47,9 @@ struct RunArgs {
     // reference evaluates them: every hypothesis against all S sources
     // (ComputeMultiViewCostVector, HPM.cu:490-495)
     unsigned long long* hyp_count;
-};
+};// Passed by value as a kernel parameter: sm_70 and later accept up to 32764 bytes.
+static_assert(sizeof(RunArgs) <= 32764, "RunArgs exceeds the kernel parameter limit");
+
 
 // Host launchers (pm_kernels.cu).  Return cudaError_t of the launch.
 cudaError_t launch_random_init(const RunArgs& a, cudaStream_t st);

@@ -124,6 +124,8 @@ int Ctx::fill_run_args(int ref, const int32_t* srcs, int n_src, const hpm_params
         a.cams[j + 1] = views[s].cam;
         a.tex[j + 1] = views[s].tex;
         hpm_view_basis(&rv.cam, &views[s].cam, a.basis[j + 1].A, a.basis[j + 1].b);
+        hpm_view_transfer(&rv.cam, &views[s].cam, a.fwd[j + 1].A, a.fwd[j + 1].b);
+        hpm_view_transfer(&views[s].cam, &rv.cam, a.bwd[j + 1].A, a.bwd[j + 1].b);
     }
     hpm_ref_kinv(&rv.cam, a.kinv);
     // 8-bit textures return grey / 255; the NCC is scale-free, only the flat-source test scales

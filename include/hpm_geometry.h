@@ -53,6 +53,55 @@ static inline void hpm_view_basis(const hpm_camera *rc, const hpm_camera *sc, fl
     b[2] = (float)((double)sc->K[8] * tr[2]);
 }
 
+/* Point transfer of the geometric consistency cost (ComputeGeomConsistencyCost,
+ * HPM.cu:539-564, through Get3DPointonWorld_cu and ProjectonCamera_cu,
+ * HPM.cu:501-537): pixel u = (x, y, 1) of camera `from` at depth d lands at
+ *     q = G u d + g,   pixel = (q_x / q_z, q_y / q_z)
+ * in camera `to`, with G = K_to R_rel Kinv_from and g = K_to t_rel.  As in the
+ * reference, the back-projection uses (x - cx) / fx, (y - cy) / fy (no skew)
+ * and the projection all nine entries of K_to.  Host only; double, rounded. */
+static inline void hpm_view_transfer(const hpm_camera *from, const hpm_camera *to, float G[9], float g[3])
+{
+    double fC[3], tC[3], Rrel[9], tr[3], M[9];
+    for (int k = 0; k < 3; ++k) {
+        fC[k] = -((double)from->R[0 + k] * from->t[0] + (double)from->R[3 + k] * from->t[1] +
+                  (double)from->R[6 + k] * from->t[2]);
+        tC[k] = -((double)to->R[0 + k] * to->t[0] + (double)to->R[3 + k] * to->t[1] + (double)to->R[6 + k] * to->t[2]);
+    }
+    for (int r = 0; r < 3; ++r) {
+        for (int k = 0; k < 3; ++k)
+            Rrel[3 * r + k] = (double)to->R[3 * r + 0] * from->R[3 * k + 0] +
+                              (double)to->R[3 * r + 1] * from->R[3 * k + 1] +
+                              (double)to->R[3 * r + 2] * from->R[3 * k + 2];
+        tr[r] = (double)to->R[3 * r + 0] * (fC[0] - tC[0]) + (double)to->R[3 * r + 1] * (fC[1] - tC[1]) +
+                (double)to->R[3 * r + 2] * (fC[2] - tC[2]);
+    }
+    const double fx = from->K[0], fy = from->K[4], cx = from->K[2], cy = from->K[5];
+    for (int r = 0; r < 3; ++r) { /* M = R_rel Kinv_from */
+        M[3 * r + 0] = Rrel[3 * r + 0] / fx;
+        M[3 * r + 1] = Rrel[3 * r + 1] / fy;
+        M[3 * r + 2] = -Rrel[3 * r + 0] * cx / fx - Rrel[3 * r + 1] * cy / fy + Rrel[3 * r + 2];
+    }
+    for (int r = 0; r < 3; ++r) {
+        for (int k = 0; k < 3; ++k)
+            G[3 * r + k] = (float)((double)to->K[3 * r + 0] * M[k] + (double)to->K[3 * r + 1] * M[3 + k] +
+                                   (double)to->K[3 * r + 2] * M[6 + k]);
+        g[r] = (float)((double)to->K[3 * r + 0] * tr[0] + (double)to->K[3 * r + 1] * tr[1] +
+                       (double)to->K[3 * r + 2] * tr[2]);
+    }
+}
+
+/* Transfer of pixel (x, y) at depth d with (G, g) of hpm_view_transfer. */
+HPM_FP_HD void hpm_transfer(const float G[9], const float g[3], float x, float y, float d, float *ox, float *oy)
+{
+    const float ax = hpm_fma(G[0], x, hpm_fma(G[1], y, G[2]));
+    const float ay = hpm_fma(G[3], x, hpm_fma(G[4], y, G[5]));
+    const float az = hpm_fma(G[6], x, hpm_fma(G[7], y, G[8]));
+    const float qz = hpm_fma(az, d, g[2]);
+    *ox = hpm_fma(ax, d, g[0]) / qz;
+    *oy = hpm_fma(ay, d, g[1]) / qz;
+}
+
 /* Entries of Kr^-1 the hypothesis term needs: 1/fx, 1/fy, cx/fx, cy/fy; host only. */
 static inline void hpm_ref_kinv(const hpm_camera *rc, float kinv[4])
 {

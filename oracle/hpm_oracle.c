@@ -27,7 +27,6 @@
 
 typedef struct { float x, y, z, w; } f4;
 typedef struct { float x, y; } f2;
-typedef struct { float x, y, z; } f3;
 
 static int g_tex_model = 0;
 void ora_set_texture_model(int model) { g_tex_model = model; }
@@ -375,50 +374,34 @@ float ora_initial_cost(const float *const *images, const hpm_camera *cams, int n
     return cost_max;
 }
 
-static f3 point_world(float x, float y, float depth, const hpm_camera *c) /* HPM.cu:501-525 */
-{
-    f3 X, T, C, R;
-    X.x = depth * (x - c->K[2]) / c->K[0];
-    X.y = depth * (y - c->K[5]) / c->K[4];
-    X.z = depth;
-    T.x = c->R[0] * X.x + c->R[3] * X.y + c->R[6] * X.z;
-    T.y = c->R[1] * X.x + c->R[4] * X.y + c->R[7] * X.z;
-    T.z = c->R[2] * X.x + c->R[5] * X.y + c->R[8] * X.z;
-    C.x = -(c->R[0] * c->t[0] + c->R[3] * c->t[1] + c->R[6] * c->t[2]);
-    C.y = -(c->R[1] * c->t[0] + c->R[4] * c->t[1] + c->R[7] * c->t[2]);
-    C.z = -(c->R[2] * c->t[0] + c->R[5] * c->t[1] + c->R[8] * c->t[2]);
-    R.x = T.x + C.x; R.y = T.y + C.y; R.z = T.z + C.z;
-    return R;
-}
-
-static void project(f3 X, const hpm_camera *c, f2 *pt, float *depth) /* HPM.cu:527-537 */
-{
-    f3 T;
-    T.x = c->R[0] * X.x + c->R[1] * X.y + c->R[2] * X.z + c->t[0];
-    T.y = c->R[3] * X.x + c->R[4] * X.y + c->R[5] * X.z + c->t[1];
-    T.z = c->R[6] * X.x + c->R[7] * X.y + c->R[8] * X.z + c->t[2];
-    *depth = c->K[6] * T.x + c->K[7] * T.y + c->K[8] * T.z;
-    pt->x = (c->K[0] * T.x + c->K[1] * T.y + c->K[2] * T.z) / *depth;
-    pt->y = (c->K[3] * T.x + c->K[4] * T.y + c->K[5] * T.z) / *depth;
-}
-
+/* ComputeGeomConsistencyCost (HPM.cu:539-564) as the point transfer of
+ * hpm_view_transfer / hpm_transfer (include/hpm_geometry.h): forward into the
+ * source at the hypothesis depth, a clamped point read of the source depth at
+ * the truncated position, back into the reference. */
 float ora_geom_cost(const float *src_depth, const hpm_camera *rc, const hpm_camera *sc,
                     const float plane[4], int px, int py)
 {
     const float max_cost = 3.0f;
     const f4 pl = { plane[0], plane[1], plane[2], plane[3] };
     const float depth = depth_from_plane(rc, pl, px, py);
-    const f3 fwd = point_world((float)px, (float)py, depth, rc);
-    f2 spt; float sd;
-    project(fwd, sc, &spt, &sd);
-    const float d = texel(src_depth, sc->width, sc->height, f2i_rz(spt.x), f2i_rz(spt.y));
+    float Gf[9], gf[3], Gb[9], gb[3];
+    hpm_view_transfer(rc, sc, Gf, gf);
+    hpm_view_transfer(sc, rc, Gb, gb);
+    float sx, sy;
+    hpm_transfer(Gf, gf, (float)px, (float)py, depth, &sx, &sy);
+    const float d = texel(src_depth, sc->width, sc->height, f2i_rz(sx), f2i_rz(sy));
     if (d == 0.0f) return max_cost;
-    const f3 sX = point_world(spt.x, spt.y, d, sc);
-    f2 bwd; float rd;
-    project(sX, rc, &bwd, &rd);
-    const float dx = px - bwd.x, dy = py - bwd.y;
+    float bx, by;
+    hpm_transfer(Gb, gb, sx, sy, d, &bx, &by);
+    const float dx = px - bx, dy = py - by;
     const float e = sqrtf(dx * dx + dy * dy);
     return (e < max_cost) ? e : max_cost; /* fminf: NaN -> 3 */
+}
+
+float ora_depth_from_plane(const hpm_camera *c, const float plane[4], int px, int py)
+{
+    const f4 pl = { plane[0], plane[1], plane[2], plane[3] };
+    return depth_from_plane(c, pl, px, py);
 }
 
 float ora_texture(const uint8_t *canny, int width, int height, int px, int py)

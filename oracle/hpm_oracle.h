@@ -8,9 +8,11 @@
  *
  * Pinning: the reference ships no tests, golden vectors or fixtures for this
  * path.  The oracle is pinned against the reference's own CUDA code built from
- * source (oracle/ref_build.mk -> oracle/_ref/libhpmref.so, run on a B200 by
- * tests/test_ref_build.py) and against the hand-derived known-answer cases in
- * tests/test_oracle.py.
+ * source (oracle/ref_build.mk -> oracle/_ref/libhpmref.so): function by
+ * function through golden vectors of its __device__ functions
+ * (tests/golden/ref_probe.npz, checked on the CPU by tests/test_golden_ref.py),
+ * whole runs statistically on a B200 (tests/test_ref_build.py), and against
+ * the hand-derived known-answer cases in tests/test_oracle.py.
  *
  * Conventions shared with the CUDA path:
  *  - images are row-major float32 grey levels (0..255), index y*width + x;
@@ -75,6 +77,9 @@ void ora_eval_costs(const float *const *images, const hpm_camera *cams, int num_
  * source depth map `src_depth` (src_cam.height x src_cam.width). */
 float ora_geom_cost(const float *src_depth, const hpm_camera *ref_cam, const hpm_camera *src_cam,
                     const float plane[4], int px, int py);
+
+/* Depth of a camera-frame plane at pixel (px, py) (ComputeDepthfromPlaneHypothesis, HPM.cu:154-157). */
+float ora_depth_from_plane(const hpm_camera *cam, const float plane[4], int px, int py);
 
 /* Multi-view initial cost and view mask (HPM.cu:450-488). */
 float ora_initial_cost(const float *const *images, const hpm_camera *cams, int num_images,

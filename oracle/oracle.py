@@ -71,6 +71,11 @@ def lib() -> ctypes.CDLL:
         L.ora_eval_costs.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int, vp, vp, vp]
         L.ora_geom_cost.restype = ctypes.c_float
         L.ora_geom_cost.argtypes = [vp, ctypes.POINTER(Camera), ctypes.POINTER(Camera), vp, ctypes.c_int, ctypes.c_int]
+        L.ora_initial_cost.restype = ctypes.c_float
+        L.ora_initial_cost.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int, ctypes.c_int, vp,
+                                       ctypes.POINTER(ctypes.c_uint32)]
+        L.ora_depth_from_plane.restype = ctypes.c_float
+        L.ora_depth_from_plane.argtypes = [ctypes.POINTER(Camera), vp, ctypes.c_int, ctypes.c_int]
         L.ora_texture.restype = ctypes.c_float
         L.ora_texture.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.ora_set_texture_model.argtypes = [ctypes.c_int]
@@ -158,6 +163,38 @@ def eval_costs(images: Sequence[np.ndarray], cams, params, px: np.ndarray, plane
     lib().ora_eval_costs(_ptr_array(imgs), cam_arr, len(imgs), ctypes.byref(prm), px.shape[0], _p(px), _p(planes),
                          _p(out))
     return out
+
+
+def initial_cost(images: Sequence[np.ndarray], cams, params, px: int, py: int, plane) -> tuple:
+    """(cost, selected-view mask) of one hypothesis (ComputeMultiViewInitialCostandSelectedViews)."""
+    imgs = [np.ascontiguousarray(i, np.float32) for i in images]
+    cam_arr = (Camera * len(cams))(*[to_cam(c) for c in cams])
+    pl = np.ascontiguousarray(plane, np.float32)
+    sel = ctypes.c_uint32(0)
+    prm = to_params(params)
+    c = lib().ora_initial_cost(_ptr_array(imgs), cam_arr, len(imgs), ctypes.byref(prm), int(px), int(py), _p(pl),
+                               ctypes.byref(sel))
+    return float(c), int(sel.value)
+
+
+def geom_cost(src_depth: np.ndarray, ref_cam, src_cam, plane, px: int, py: int) -> float:
+    """Geometric consistency cost of one hypothesis against one source depth map."""
+    d = np.ascontiguousarray(src_depth, np.float32)
+    pl = np.ascontiguousarray(plane, np.float32)
+    rc, sc = to_cam(ref_cam), to_cam(src_cam)
+    return float(lib().ora_geom_cost(_p(d), ctypes.byref(rc), ctypes.byref(sc), _p(pl), int(px), int(py)))
+
+
+def depth_from_plane(cam, plane, px: int, py: int) -> float:
+    pl = np.ascontiguousarray(plane, np.float32)
+    c = to_cam(cam)
+    return float(lib().ora_depth_from_plane(ctypes.byref(c), _p(pl), int(px), int(py)))
+
+
+def texture(canny: np.ndarray, px: int, py: int) -> float:
+    """Edge-density texture term at (px, py) of a 0 / non-zero edge map."""
+    e = np.ascontiguousarray(canny, np.uint8)
+    return float(lib().ora_texture(_p(e), e.shape[1], e.shape[0], int(px), int(py)))
 
 
 class RunState:

@@ -37,6 +37,9 @@ def lib() -> ctypes.CDLL:
         _lib.ref_run_patchmatch.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ora.Params), vp, vp, vp, vp, vp,
                                             vp, vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32,
                                             ctypes.POINTER(ctypes.c_float)]
+        _lib.ref_probe.restype = ctypes.c_int
+        _lib.ref_probe.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(ora.Params), vp, vp, vp, ctypes.c_int,
+                                   ctypes.c_int, vp, vp, vp, vp, vp, vp]
     return _lib
 
 
@@ -62,3 +65,32 @@ def run_patchmatch(images, depths, cams, params, st: "ora.RunState", seed: int, 
     if rc != 0:
         raise RuntimeError(f"reference build: CUDA error {rc}")
     return float(ms.value)
+
+
+def probe(images, depths, cams, params, canny, pix, planes, address_mode: int = 0) -> dict:
+    """The reference's own per-pixel functions at given (pixel, camera-frame plane)
+    pairs: ComputeMultiViewCostVector, ComputeMultiViewInitialCostandSelectedViews,
+    ComputeDepthfromPlaneHypothesis, ComputeGeomConsistencyCost against every
+    source's depth map and ComputeTexture (HPM.cu:154-564).  address_mode 0 =
+    clamp, 1 = wrap for the image and depth textures."""
+    imgs = [np.ascontiguousarray(i, np.float32) for i in images]
+    deps = [np.ascontiguousarray(d, np.float32) for d in depths]
+    cam_arr = (ora.Camera * len(cams))(*[ora.to_cam(c) for c in cams])
+    prm = ora.to_params(params)
+    can = np.ascontiguousarray(canny, np.uint32)
+    px = np.ascontiguousarray(pix, np.int32).reshape(-1, 2)
+    pl = np.ascontiguousarray(planes, np.float32).reshape(-1, 4)
+    n = px.shape[0]
+    out = {"cost_vec": np.zeros((n, 32), np.float32), "init_cost": np.zeros(n, np.float32),
+           "selected": np.zeros(n, np.uint32), "depth": np.zeros(n, np.float32),
+           "geom": np.zeros((n, 32), np.float32), "texture": np.zeros(n, np.float32)}
+    rc = lib().ref_probe(_ptrs(imgs), _ptrs(deps), cam_arr, len(imgs), ctypes.byref(prm), can.ctypes.data,
+                         px.ctypes.data, pl.ctypes.data, n, address_mode, out["cost_vec"].ctypes.data,
+                         out["init_cost"].ctypes.data, out["selected"].ctypes.data, out["depth"].ctypes.data,
+                         out["geom"].ctypes.data, out["texture"].ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"reference build: probe failed ({rc})")
+    S = len(imgs) - 1
+    out["cost_vec"] = out["cost_vec"][:, :S].copy()
+    out["geom"] = out["geom"][:, :S].copy()
+    return out

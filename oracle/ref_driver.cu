@@ -71,7 +71,8 @@ struct RefParams {
     unsigned int mode;  // hpm_types.h HPM_MODE_* bits
 };
 
-static void make_texture(const float* host, int w, int h, cudaArray** arr, cudaTextureObject_t* tex) {
+static void make_texture(const float* host, int w, int h, cudaArray** arr, cudaTextureObject_t* tex,
+                         cudaTextureAddressMode mode = cudaAddressModeWrap) {
     cudaChannelFormatDesc fd = cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat);
     cudaMallocArray(arr, &fd, w, h);
     cudaMemcpy2DToArray(*arr, 0, 0, host, sizeof(float) * w, sizeof(float) * w, h, cudaMemcpyHostToDevice);
@@ -81,24 +82,15 @@ static void make_texture(const float* host, int w, int h, cudaArray** arr, cudaT
     rd.res.array.array = *arr;
     cudaTextureDesc td;
     memset(&td, 0, sizeof(td));
-    td.addressMode[0] = cudaAddressModeWrap;
-    td.addressMode[1] = cudaAddressModeWrap;
+    td.addressMode[0] = mode;
+    td.addressMode[1] = mode;
     td.filterMode = cudaFilterModeLinear;
     td.readMode = cudaReadModeElementType;
     td.normalizedCoords = 0;
     cudaCreateTextureObject(tex, &rd, &td, nullptr);
 }
 
-extern "C" int ref_run_patchmatch(const float* const* images, const Camera* cams, int num_images, const RefParams* rp,
-                                  float* planes, float* costs, const float* scaled_planes, const float* prior_planes,
-                                  const unsigned int* plane_masks, float* confidences, const unsigned int* canny,
-                                  float* texture, const float* const* depth_maps, unsigned long long seed,
-                                  unsigned int view, float* elapsed_ms) {
-    (void)cudaGetLastError();
-    HPM hpm;
-    const int W = cams[0].width, H = cams[0].height;
-    const size_t n = (size_t)W * H;
-    PatchMatchParams& p = hpm.params;
+static void fill_params(PatchMatchParams& p, const RefParams* rp, int num_images) {
     p.max_iterations = rp->max_iterations;
     p.patch_size = rp->patch_size;
     p.num_images = num_images;
@@ -116,6 +108,19 @@ extern "C" int ref_run_patchmatch(const float* const* images, const Camera* cams
     p.hierarchy = rp->mode & 8u;
     p.upsample = rp->mode & 16u;
     p.mand_consistency = rp->mode & 32u;
+}
+
+extern "C" int ref_run_patchmatch(const float* const* images, const Camera* cams, int num_images, const RefParams* rp,
+                                  float* planes, float* costs, const float* scaled_planes, const float* prior_planes,
+                                  const unsigned int* plane_masks, float* confidences, const unsigned int* canny,
+                                  float* texture, const float* const* depth_maps, unsigned long long seed,
+                                  unsigned int view, float* elapsed_ms) {
+    (void)cudaGetLastError();
+    HPM hpm;
+    const int W = cams[0].width, H = cams[0].height;
+    const size_t n = (size_t)W * H;
+    PatchMatchParams& p = hpm.params;
+    fill_params(p, rp, num_images);
     hpm.num_images = num_images;
     hpm.cameras.assign(cams, cams + num_images);
     for (int i = 0; i < num_images; ++i)
@@ -184,5 +189,120 @@ extern "C" int ref_run_patchmatch(const float* const* images, const Camera* cams
     const cudaError_t err = cudaDeviceSynchronize();
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    return err == cudaSuccess ? 0 : (int)err;
+}
+
+// ---------------------------------------------------------------------------
+// Per-function probes: the reference's own __device__ functions (HPM.cu,
+// linked through -rdc) evaluated at given (pixel, hypothesis) pairs, for the
+// golden vectors that pin the oracle function by function.
+__device__ void ComputeMultiViewCostVector(const cudaTextureObject_t* images, const Camera* cameras, const int2 p,
+                                           const float4 plane_hypothesis, float* cost_vector,
+                                           const PatchMatchParams params);
+__device__ float ComputeMultiViewInitialCostandSelectedViews(const cudaTextureObject_t* images, const Camera* cameras,
+                                                             const int2 p, const float4 plane_hypothesis,
+                                                             unsigned int* selected_views,
+                                                             const PatchMatchParams params);
+__device__ float ComputeGeomConsistencyCost(const cudaTextureObject_t depth_image, const Camera ref_camera,
+                                            const Camera src_camera, const float4 plane_hypothesis, const int2 p);
+__device__ float ComputeDepthfromPlaneHypothesis(const Camera camera, const float4 plane_hypothesis, const int2 p);
+__device__ float ComputeTexture(const unsigned int* Canny, const Camera* cameras, const int2 p);
+
+// One thread per probe; cost_vec and geom hold 32 entries per probe (sources in order).
+__global__ void k_ref_probe(const cudaTextureObjects* tex, const cudaTextureObjects* dtex, const Camera* cams,
+                            const PatchMatchParams p, const unsigned int* canny, const int2* pix, const float4* planes,
+                            int n, float* cost_vec, float* init_cost, unsigned int* sel, float* depth, float* geom,
+                            float* texture) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int2 q = pix[i];
+    const float4 pl = planes[i];
+    float cv[32];
+    ComputeMultiViewCostVector(tex->images, cams, q, pl, cv, p);
+    for (int j = 0; j < p.num_images - 1; ++j) cost_vec[32 * i + j] = cv[j];
+    unsigned int s = 0;
+    init_cost[i] = ComputeMultiViewInitialCostandSelectedViews(tex->images, cams, q, pl, &s, p);
+    sel[i] = s;
+    depth[i] = ComputeDepthfromPlaneHypothesis(cams[0], pl, q);
+    for (int j = 1; j < p.num_images; ++j)
+        geom[32 * i + j - 1] = ComputeGeomConsistencyCost(dtex->images[j], cams[0], cams[j], pl, q);
+    texture[i] = ComputeTexture(canny, cams, q);
+}
+
+// images / depth_maps: num_images float maps of each camera's size; canny: the
+// reference's width*height; pix: n int2 inside the reference image; planes: n
+// float4 (camera frame).  address_mode 0 = clamp, 1 = wrap (the reference's
+// HPM.cpp:759-768).
+extern "C" int ref_probe(const float* const* images, const float* const* depth_maps, const Camera* cams,
+                         int num_images, const RefParams* rp, const unsigned int* canny, const int* pix,
+                         const float* planes, int n, int address_mode, float* cost_vec, float* init_cost,
+                         unsigned int* sel, float* depth, float* geom, float* texture) {
+    (void)cudaGetLastError();
+    if (num_images < 2 || num_images > 33 || n <= 0) return -1;
+    const int W = cams[0].width, H = cams[0].height;
+    for (int i = 0; i < n; ++i)
+        if (pix[2 * i] < 0 || pix[2 * i] >= W || pix[2 * i + 1] < 0 || pix[2 * i + 1] >= H) return -2;
+    const cudaTextureAddressMode mode = address_mode ? cudaAddressModeWrap : cudaAddressModeClamp;
+    cudaTextureObjects th, dh;
+    memset(&th, 0, sizeof(th));
+    memset(&dh, 0, sizeof(dh));
+    std::vector<cudaArray*> arrs(2 * num_images, nullptr);
+    for (int i = 0; i < num_images; ++i) {
+        make_texture(images[i], cams[i].width, cams[i].height, &arrs[i], &th.images[i], mode);
+        make_texture(depth_maps[i], cams[i].width, cams[i].height, &arrs[num_images + i], &dh.images[i], mode);
+    }
+    PatchMatchParams p;
+    memset(&p, 0, sizeof(p));
+    fill_params(p, rp, num_images);
+    const size_t wh = (size_t)W * H;
+    cudaTextureObjects *dt = nullptr, *dd = nullptr;
+    Camera* dc = nullptr;
+    unsigned int *dcanny = nullptr, *dsel = nullptr;
+    int2* dpix = nullptr;
+    float4* dpl = nullptr;
+    float *dcv = nullptr, *dic = nullptr, *ddep = nullptr, *dgeom = nullptr, *dtexo = nullptr;
+    cudaMalloc((void**)&dt, sizeof(th));
+    cudaMalloc((void**)&dd, sizeof(dh));
+    cudaMalloc((void**)&dc, sizeof(Camera) * num_images);
+    cudaMalloc((void**)&dcanny, sizeof(unsigned int) * wh);
+    cudaMalloc((void**)&dpix, sizeof(int2) * n);
+    cudaMalloc((void**)&dpl, sizeof(float4) * n);
+    cudaMalloc((void**)&dcv, sizeof(float) * 32 * n);
+    cudaMalloc((void**)&dic, sizeof(float) * n);
+    cudaMalloc((void**)&dsel, sizeof(unsigned int) * n);
+    cudaMalloc((void**)&ddep, sizeof(float) * n);
+    cudaMalloc((void**)&dgeom, sizeof(float) * 32 * n);
+    cudaMalloc((void**)&dtexo, sizeof(float) * n);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) {
+        cudaMemcpy(dt, &th, sizeof(th), cudaMemcpyHostToDevice);
+        cudaMemcpy(dd, &dh, sizeof(dh), cudaMemcpyHostToDevice);
+        cudaMemcpy(dc, cams, sizeof(Camera) * num_images, cudaMemcpyHostToDevice);
+        cudaMemcpy(dcanny, canny, sizeof(unsigned int) * wh, cudaMemcpyHostToDevice);
+        cudaMemcpy(dpix, pix, sizeof(int2) * n, cudaMemcpyHostToDevice);
+        cudaMemcpy(dpl, planes, sizeof(float4) * n, cudaMemcpyHostToDevice);
+        cudaMemset(dcv, 0, sizeof(float) * 32 * n);
+        cudaMemset(dgeom, 0, sizeof(float) * 32 * n);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) {
+        k_ref_probe<<<(n + 127) / 128, 128>>>(dt, dd, dc, p, dcanny, dpix, dpl, n, dcv, dic, dsel, ddep, dgeom, dtexo);
+        err = cudaDeviceSynchronize();
+    }
+    if (err == cudaSuccess) {
+        cudaMemcpy(cost_vec, dcv, sizeof(float) * 32 * n, cudaMemcpyDeviceToHost);
+        cudaMemcpy(init_cost, dic, sizeof(float) * n, cudaMemcpyDeviceToHost);
+        cudaMemcpy(sel, dsel, sizeof(unsigned int) * n, cudaMemcpyDeviceToHost);
+        cudaMemcpy(depth, ddep, sizeof(float) * n, cudaMemcpyDeviceToHost);
+        cudaMemcpy(geom, dgeom, sizeof(float) * 32 * n, cudaMemcpyDeviceToHost);
+        err = cudaMemcpy(texture, dtexo, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    }
+    void* bufs[] = {dt, dd, dc, dcanny, dpix, dpl, dcv, dic, dsel, ddep, dgeom, dtexo};
+    for (void* b : bufs) cudaFree(b);
+    for (int i = 0; i < num_images; ++i) {
+        cudaDestroyTextureObject(th.images[i]);
+        cudaDestroyTextureObject(dh.images[i]);
+    }
+    for (cudaArray* a : arrs) cudaFreeArray(a);
     return err == cudaSuccess ? 0 : (int)err;
 }

@@ -1,0 +1,132 @@
+"""Generates tests/golden/ref_probe.npz: golden vectors of the reference's own
+per-pixel functions (HPM.cu of HPM-MVS++, compiled from its sources by
+oracle/ref_build.mk into oracle/_ref/libhpmref.so) at fixed (pixel, plane)
+pairs of a small seeded synthetic scene.
+
+Needs a CUDA device and the reference build; run from the repository root:
+
+    python tests/golden/make_ref_golden.py [--out tests/golden/ref_probe.npz]
+
+The functions probed (HPM.cu line ranges):
+  ComputeMultiViewCostVector                      490-495  per-source bilateral NCC
+  ComputeMultiViewInitialCostandSelectedViews     450-488  top-k cost and view mask
+  ComputeDepthfromPlaneHypothesis                 154-157
+  ComputeGeomConsistencyCost                      539-564  against each source's depth map
+  ComputeTexture                                  349-373
+
+The scene is 5 views of 128x96 (seed 11, 4 sources).  Its grey images are
+integers (stored as uint8) and its depth maps are the ground truth rounded to
+1/256 (stored as uint16 counts of 1/256), so the stored inputs are exactly
+the inputs the reference saw.  Textures use clamp addressing (address_mode 0),
+the convention of the CUDA path and the oracle; the reference's host code
+selects wrap (HPM.cpp:759-768), which changes only fetches outside the image.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import conftest  # noqa: E402  (registers hpm_b200 and hpm_oracle)
+
+W, H, N_VIEWS, SEED = 128, 96, 5, 11
+N_PROBES = 1536
+
+
+def camera_frame_plane(K, R, n_world, depth, px, py):
+    """(n_c, w) with n_c = R n_world and w = -n_c . X, X the camera-frame point at depth."""
+    n = R @ n_world
+    X = depth * np.array([(px - K[0, 2]) / K[0, 0], (py - K[1, 2]) / K[1, 1], 1.0])
+    return np.array([n[0], n[1], n[2], -float(n @ X)])
+
+
+def make_inputs() -> dict:
+    """Scene, probe pixels and planes: one third ground-truth planes, one third
+    perturbed ones (normal noise 0.15, depth within 5 %), the rest random planes
+    facing the camera (and every probe on the background)."""
+    import cv2
+    import hpm_b200
+    from hpm_b200 import synth
+
+    scene = synth.make_scene(n_views=N_VIEWS, width=W, height=H, seed=SEED, n_src=N_VIEWS - 1)
+    order = [0] + [j for j, _ in scene.pairs[0]]
+    views = [scene.views[i] for i in order]
+    grays = np.stack([synth.gray_float(v.image).astype(np.uint8) for v in views])
+    depth_q = np.stack([np.round(v.depth.astype(np.float64) * 256.0).astype(np.uint16) for v in views])
+    canny = (cv2.Canny(views[0].image, 50, 150) > 0).astype(np.uint8)
+    rng = np.random.default_rng(SEED)
+    v0 = views[0]
+    K, R = v0.K.astype(np.float64), v0.R.astype(np.float64)
+    cam0 = conftest.scene_cams(scene)[0]
+    dmin, dmax = hpm_b200.widened_range(cam0)
+    pix = np.stack([rng.integers(0, W, N_PROBES), rng.integers(0, H, N_PROBES)], axis=1).astype(np.int32)
+    planes = np.zeros((N_PROBES, 4), np.float64)
+    kind = np.zeros(N_PROBES, np.int8)  # 0 ground truth, 1 perturbed, 2 random
+    for k in range(N_PROBES):
+        px, py = int(pix[k, 0]), int(pix[k, 1])
+        d = float(v0.depth[py, px])
+        kind[k] = k % 3 if d > 0 else 2
+        if kind[k] == 0:
+            planes[k] = camera_frame_plane(K, R, v0.normal[py, px].astype(np.float64), d, px, py)
+        elif kind[k] == 1:
+            nw = v0.normal[py, px].astype(np.float64) + rng.normal(0.0, 0.15, 3)
+            nw /= np.linalg.norm(nw)
+            planes[k] = camera_frame_plane(K, R, nw, d * rng.uniform(0.95, 1.05), px, py)
+        else:
+            n = rng.normal(0.0, 1.0, 3)
+            n[2] = -abs(n[2]) - 0.3
+            n /= np.linalg.norm(n)
+            X = rng.uniform(dmin, dmax) * np.array([(px - K[0, 2]) / K[0, 0], (py - K[1, 2]) / K[1, 1], 1.0])
+            planes[k] = np.array([n[0], n[1], n[2], -float(n @ X)])
+    return dict(
+        images=grays, depth_q=depth_q, canny=canny,
+        K=np.stack([v.K for v in views]).astype(np.float32), R=np.stack([v.R for v in views]).astype(np.float32),
+        t=np.stack([v.t for v in views]).astype(np.float32),
+        depth_min=np.array([v.depth_min for v in views], np.float32),
+        depth_max=np.array([v.depth_max for v in views], np.float32),
+        range=np.array([dmin, dmax], np.float32),
+        pix=pix, planes=planes.astype(np.float32), kind=kind, address_mode=np.int32(0))
+
+
+def load(path: str):
+    """The stored inputs as the functions take them: (grey float images, depth
+    maps, cameras, params) plus the whole archive as a dict."""
+    import hpm_b200
+
+    z = dict(np.load(path))
+    images = [im.astype(np.float32) for im in z["images"]]
+    depths = [(d.astype(np.float64) / 256.0).astype(np.float32) for d in z["depth_q"]]
+    cams = [hpm_b200.Camera.make(z["K"][i], z["R"][i], z["t"][i], W, H, float(z["depth_min"][i]),
+                                 float(z["depth_max"][i])) for i in range(len(images))]
+    params = hpm_b200.Params.make(len(images), float(z["range"][0]), float(z["range"][1]))
+    return images, depths, cams, params, z
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.join(HERE, "ref_probe.npz"))
+    args = ap.parse_args()
+    import ref_cuda
+
+    if not ref_cuda.available():
+        raise SystemExit("oracle/_ref/libhpmref.so is not built (make -C oracle -f ref_build.mk)")
+    inputs = make_inputs()
+    tmp = args.out + ".inputs.npz"
+    np.savez_compressed(tmp, **inputs)
+    images, depths, cams, params, z = load(tmp)
+    os.remove(tmp)
+    out = ref_cuda.probe(images, depths, cams, params, z["canny"].astype(np.uint32), z["pix"], z["planes"],
+                         address_mode=int(z["address_mode"]))
+    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+    np.savez_compressed(args.out, **inputs, **{"ref_" + k: v for k, v in out.items()})
+    print(f"wrote {args.out}: {len(z['pix'])} probes, {len(images) - 1} sources")
+
+
+if __name__ == "__main__":
+    main()
