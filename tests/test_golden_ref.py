@@ -1,0 +1,241 @@
+"""The oracle against golden vectors of the reference's own per-pixel functions.
+
+tests/golden/ref_probe.npz holds the outputs of HPM.cu's
+ComputeMultiViewCostVector, ComputeMultiViewInitialCostandSelectedViews,
+ComputeDepthfromPlaneHypothesis, ComputeGeomConsistencyCost and ComputeTexture
+(the reference compiled from its sources for sm_100a, with its own
+--use_fast_math flags) at 1536 (pixel, plane) pairs of a seeded 5-view scene,
+with the inputs they saw; tests/golden/make_ref_golden.py made it.
+
+The oracle is IEEE float and evaluates the homography in factored form, so it
+cannot equal fast-math output bit for bit.  What is checked is that every
+difference is of the size float32 rounding explains:
+
+- on textured patches, costs agree to 2e-4 at 99 % of (probe, source) pairs
+  and to 1.5e-3 everywhere (a sample position that moves by a few ulps can
+  cross one of the texture unit's 1/256 weight steps);
+- on patches of pure noise (the scene's background: grey about 190, sigma 2)
+  the reference's variance E[x^2] - E[x]^2 cancels catastrophically, and the
+  difference stays within 16 unit roundoffs of the magnitudes that cancel
+  (ncc_rounding_scale, computed in FP64 from the same samples);
+- hypotheses whose plane is within 6 degrees of edge-on to the pixel's ray
+  (|cos| < 0.1) make the homography nearly singular, so the positions of the
+  two evaluations differ by far more than rounding; they are counted, not
+  compared;
+- discrete decisions (a view at the top-k threshold, a truncated texel index)
+  may differ only where the compared quantities sit at the decision boundary.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import hpm_oracle as ora  # noqa: E402
+import make_ref_golden as golden  # noqa: E402
+
+FIXTURE = os.path.join(HERE, "golden", "ref_probe.npz")
+
+U = 2.0 ** -24        # float32 unit roundoff
+TOL_NCC = 2e-4        # per-source bilateral NCC cost, range [0, 2]: 99 % of textured pairs
+TOL_NCC_MAX = 1.5e-3  # every pair that is not edge-on, unless the rounding scale allows more
+K_NCC = 16            # unit roundoffs of the cancelling magnitudes
+MIN_COS = 0.1         # edge-on limit |cos(normal, ray)|
+TOL_DEPTH_REL = 2e-6  # depth of a plane, unless its denominator cancels
+TOL_GEOM = 2e-3       # reprojection distance in pixels, range [0, 3]
+TOL_TEXTURE_REL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def probe():
+    assert os.path.exists(FIXTURE), "tests/golden/ref_probe.npz is missing (tests/golden/make_ref_golden.py)"
+    return golden.load(FIXTURE)
+
+
+def _mat(cam, field, shape):
+    return np.array(getattr(cam, field), np.float64).reshape(shape)
+
+
+def homography64(rc, sc, plane):
+    """ComputeHomography (HPM.cu:251-311) in float64: Ks' (R_rel - t_rel n^T / d) Kr^-1."""
+    Kr, Rr, tr = _mat(rc, "K", (3, 3)), _mat(rc, "R", (3, 3)), _mat(rc, "t", (3,))
+    Ks, Rs, ts = _mat(sc, "K", (3, 3)), _mat(sc, "R", (3, 3)), _mat(sc, "t", (3,))
+    Rrel = Rs @ Rr.T
+    trel = Rs @ (-Rr.T @ tr + Rs.T @ ts)
+    Ksp = np.array([[Ks[0, 0], 0, Ks[0, 2]], [0, Ks[1, 1], Ks[1, 2]], [0, 0, Ks[2, 2]]])
+    Kri = np.array([[1 / Kr[0, 0], 0, -Kr[0, 2] / Kr[0, 0]], [0, 1 / Kr[1, 1], -Kr[1, 2] / Kr[1, 1]], [0, 0, 1]])
+    n = np.asarray(plane[:3], np.float64)
+    return Ksp @ (Rrel - np.outer(trel, n) / float(plane[3])) @ Kri
+
+
+def _bilinear(img, x, y):
+    h, w = img.shape
+    x0, y0 = np.floor(x), np.floor(y)
+    fx, fy = x - x0, y - y0
+
+    def at(xx, yy):
+        return img[np.clip(yy, 0, h - 1).astype(int), np.clip(xx, 0, w - 1).astype(int)]
+
+    return ((1 - fx) * (1 - fy) * at(x0, y0) + fx * (1 - fy) * at(x0 + 1, y0) + (1 - fx) * fy * at(x0, y0 + 1) +
+            fx * fy * at(x0 + 1, y0 + 1))
+
+
+def ncc_rounding_scale(images, cams, params, pix, planes) -> np.ndarray:
+    """Per (probe, source): u * (|S_rs| + |S_r S_s|) / sqrt(v_r v_s)
+    + |ncc| / 2 * ((S_rr + S_r^2) / v_r + (S_ss + S_s^2) / v_s), from the
+    bilateral sums of HPM.cu:388-446 evaluated in FP64 (exact bilinear).  It is
+    the first-order effect on the cost of one unit roundoff in each cancelling
+    sum; 0 where the centre projects outside the source (cost 2 in both), inf
+    where a variance is below 1e-3 (the 1e-5 floor is then within reach)."""
+    r = params.patch_size // 2
+    off = np.arange(-r, r + 1, params.radius_increment, dtype=np.float64)
+    ii, jj = (a.ravel() for a in np.meshgrid(off, off, indexing="ij"))
+    out = np.zeros((len(pix), len(images) - 1))
+    ref = images[0].astype(np.float64)
+    h0, w0 = ref.shape
+    for k, ((px, py), pl) in enumerate(zip(pix, planes)):
+        rx, ry = np.clip(px + ii, 0, w0 - 1).astype(int), np.clip(py + jj, 0, h0 - 1).astype(int)
+        rv = ref[ry, rx]
+        w = np.exp(-np.sqrt(ii * ii + jj * jj) / (2 * params.sigma_spatial ** 2) -
+                   np.abs(rv - ref[py, px]) / (2 * params.sigma_color ** 2))
+        w /= w.sum()
+        for j in range(len(images) - 1):
+            Hm = homography64(cams[0], cams[j + 1], pl)
+            src = images[j + 1].astype(np.float64)
+            c = Hm @ np.array([px, py, 1.0])
+            if not (0 <= c[0] / c[2] < src.shape[1] and 0 <= c[1] / c[2] < src.shape[0]):
+                continue
+            X, Y = px + ii, py + jj
+            den = Hm[2, 0] * X + Hm[2, 1] * Y + Hm[2, 2]
+            sv = _bilinear(src, (Hm[0, 0] * X + Hm[0, 1] * Y + Hm[0, 2]) / den,
+                           (Hm[1, 0] * X + Hm[1, 1] * Y + Hm[1, 2]) / den)
+            Sr, Srr, Ss, Sss, Srs = (w * rv).sum(), (w * rv * rv).sum(), (w * sv).sum(), (w * sv * sv).sum(), \
+                (w * rv * sv).sum()
+            vr, vs = Srr - Sr * Sr, Sss - Ss * Ss
+            if vr < 1e-3 or vs < 1e-3:
+                out[k, j] = np.inf
+                continue
+            ncc = (Srs - Sr * Ss) / np.sqrt(vr * vs)
+            out[k, j] = U * ((abs(Srs) + abs(Sr * Ss)) / np.sqrt(vr * vs) +
+                             abs(ncc) / 2 * ((Srr + Sr * Sr) / vr + (Sss + Ss * Ss) / vs))
+    return out
+
+
+def edge_on(cams, pix, planes) -> np.ndarray:
+    """|cos| between the plane normal and the pixel's viewing ray below MIN_COS."""
+    K = _mat(cams[0], "K", (3, 3))
+    ray = np.stack([(pix[:, 0] - K[0, 2]) / K[0, 0], (pix[:, 1] - K[1, 2]) / K[1, 1], np.ones(len(pix))], 1)
+    n = planes[:, :3].astype(np.float64)
+    cos = np.abs((n * ray).sum(1)) / (np.linalg.norm(n, axis=1) * np.linalg.norm(ray, axis=1))
+    return cos < MIN_COS
+
+
+def ncc_allowance(images, depths, cams, params, z):
+    """(allowed |difference| per (probe, source), textured mask, edge-on mask)."""
+    scale = ncc_rounding_scale(images, cams, params, z["pix"], z["planes"])
+    allow = np.maximum(TOL_NCC_MAX, K_NCC * scale)
+    textured = (depths[0][z["pix"][:, 1], z["pix"][:, 0]] > 0)[:, None] & np.ones((1, scale.shape[1]), bool)
+    return allow, textured, edge_on(cams, z["pix"], z["planes"])
+
+
+def check_costs(got, ref, allow, textured, edge):
+    """The assertions shared by the oracle and the CUDA path."""
+    keep = ~edge[:, None] & np.ones((1, got.shape[1]), bool)
+    d = np.abs(got - ref)
+    bad = keep & (d > allow)
+    assert not bad.any(), [(int(k), int(j), float(d[k, j]), float(allow[k, j])) for k, j in np.argwhere(bad)[:5]]
+    assert (d[keep & textured] <= TOL_NCC).mean() >= 0.99
+    assert np.median(d[keep]) <= 1e-5
+    assert edge.mean() <= 0.15  # the excluded share stays small
+
+
+def test_fixture_covers_every_case(probe):
+    _, _, _, _, z = probe
+    assert np.bincount(z["kind"], minlength=3).min() >= 300
+    assert (z["ref_cost_vec"] >= 2.0).any() and (z["ref_cost_vec"] < 0.2).any()
+    assert (z["ref_geom"] == 3.0).any() and (z["ref_geom"] < 0.5).any()
+    assert (z["ref_texture"] < 0.9).any() and (z["ref_texture"] > 0.99).any()
+
+
+def test_ncc_cost_vector_matches_reference(probe):
+    images, depths, cams, params, z = probe
+    got = ora.eval_costs(images, cams, params, z["pix"], z["planes"])
+    allow, textured, edge = ncc_allowance(images, depths, cams, params, z)
+    check_costs(got, z["ref_cost_vec"], allow, textured, edge)
+
+
+def test_initial_cost_and_view_mask_match_reference(probe):
+    images, depths, cams, params, z = probe
+    allow, _, edge = ncc_allowance(images, depths, cams, params, z)
+    ref_cv = z["ref_cost_vec"]
+    for k in np.nonzero(~edge)[0]:
+        c, sel = ora.initial_cost(images, cams, params, *z["pix"][k], z["planes"][k])
+        a = allow[k].max()
+        assert abs(c - z["ref_init_cost"][k]) <= a, (k, c, float(z["ref_init_cost"][k]))
+        if sel != z["ref_selected"][k]:
+            # only a view whose cost sits at the top-k threshold may differ
+            valid = ref_cv[k][ref_cv[k] < 2.0]
+            thr = np.sort(valid)[: params.top_k].max()
+            diff = sel ^ int(z["ref_selected"][k])
+            for j in range(ref_cv.shape[1]):
+                if diff >> j & 1:
+                    assert abs(ref_cv[k][j] - thr) <= 2 * a, (k, j)
+
+
+def test_depth_from_plane_matches_reference(probe):
+    _, _, cams, _, z = probe
+    K = _mat(cams[0], "K", (3, 3))
+    pl = z["planes"].astype(np.float64)
+    px, py = z["pix"][:, 0].astype(np.float64), z["pix"][:, 1].astype(np.float64)
+    terms = np.abs(np.stack([(px - K[0, 2]) * pl[:, 0], K[0, 0] / K[1, 1] * (py - K[1, 2]) * pl[:, 1],
+                             K[0, 0] * pl[:, 2]], 1))
+    den = (px - K[0, 2]) * pl[:, 0] + K[0, 0] / K[1, 1] * (py - K[1, 2]) * pl[:, 1] + K[0, 0] * pl[:, 2]
+    allow = np.maximum(TOL_DEPTH_REL, 8 * U * terms.sum(1) / np.abs(den))
+    got = np.array([ora.depth_from_plane(cams[0], z["planes"][k], *z["pix"][k]) for k in range(len(z["pix"]))])
+    ref = z["ref_depth"].astype(np.float64)
+    rel = np.abs(got - ref) / np.abs(ref)
+    assert (rel <= allow).all(), np.argwhere(rel > allow)[:5].ravel()
+    assert np.quantile(rel, 0.99) <= TOL_DEPTH_REL
+
+
+def _forward_pixel64(cam_r, cam_s, plane, px, py):
+    """Float64 forward transfer of the geometric cost (HPM.cu:543-548)."""
+    K, R, t = _mat(cam_r, "K", (3, 3)), _mat(cam_r, "R", (3, 3)), _mat(cam_r, "t", (3,))
+    Ks, Rs, ts = _mat(cam_s, "K", (3, 3)), _mat(cam_s, "R", (3, 3)), _mat(cam_s, "t", (3,))
+    n = np.asarray(plane[:3], np.float64)
+    den = (px - K[0, 2]) * n[0] + (K[0, 0] / K[1, 1]) * (py - K[1, 2]) * n[1] + K[0, 0] * n[2]
+    depth = -float(plane[3]) * K[0, 0] / den
+    Xc = depth * np.array([(px - K[0, 2]) / K[0, 0], (py - K[1, 2]) / K[1, 1], 1.0])
+    q = Ks @ (Rs @ (R.T @ (Xc - t)) + ts)
+    return q[0] / q[2], q[1] / q[2]
+
+
+def test_geometric_cost_matches_reference(probe):
+    _, depths, cams, _, z = probe
+    ref = z["ref_geom"]
+    boundary = 0
+    for k in range(len(z["pix"])):
+        px, py = (int(v) for v in z["pix"][k])
+        for j in range(ref.shape[1]):
+            got = ora.geom_cost(depths[j + 1], cams[0], cams[j + 1], z["planes"][k], px, py)
+            if abs(got - ref[k, j]) <= TOL_GEOM:
+                continue
+            # otherwise the source texel index must sit on a truncation boundary
+            sx, sy = _forward_pixel64(cams[0], cams[j + 1], z["planes"][k], px, py)
+            near = min(abs(sx - round(sx)), abs(sy - round(sy)))
+            assert near <= 1e-3, (k, j, got, float(ref[k, j]), sx, sy)
+            boundary += 1
+    assert boundary <= 0.002 * ref.size, boundary
+
+
+def test_texture_term_matches_reference(probe):
+    _, _, _, _, z = probe
+    got = np.array([ora.texture(z["canny"], *z["pix"][k]) for k in range(len(z["pix"]))])
+    ref = z["ref_texture"].astype(np.float64)
+    rel = np.abs(got - ref) / np.abs(ref)
+    assert rel.max() <= TOL_TEXTURE_REL, rel.max()
