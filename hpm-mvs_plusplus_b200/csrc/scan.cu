@@ -306,30 +306,64 @@ __global__ void k_fuse_emit(const ScanView* __restrict__ views, int i, const int
     out[k] = p;
 }
 
-// exclusive prefix sum of keep flags (single block, serial over chunks)
-__global__ void k_exclusive_sum(const int32_t* __restrict__ in, int32_t* __restrict__ out, int n,
-                                int32_t* __restrict__ total) {
-    __shared__ int32_t s[kScanBlock];
-    __shared__ int32_t carry;
-    if (threadIdx.x == 0) carry = 0;
+// Compaction offsets of the fused points: an exclusive prefix sum of the keep
+// flags in three launches over tiles of kScanBlock pixels -- tile totals, an
+// exclusive scan of the totals (one block), and each tile's scan plus its
+// offset.  Warp scans by shuffle, then a scan of the 32 warp totals.
+__device__ __forceinline__ int32_t warp_inclusive_sum(int32_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Inclusive sum over a block of kScanBlock threads; ws[31] holds the block
+// total when it returns.  The caller syncs before ws is written again.
+__device__ __forceinline__ int32_t block_inclusive_sum(int32_t v, int32_t* ws) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    v = warp_inclusive_sum(v);
+    if (lane == 31) ws[w] = v;
     __syncthreads();
-    for (int base = 0; base < n; base += kScanBlock) {
+    if (w == 0) ws[lane] = warp_inclusive_sum(ws[lane]);
+    __syncthreads();
+    return v + (w > 0 ? ws[w - 1] : 0);
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_tile_sums(const int32_t* __restrict__ in, int n,
+                                                          int32_t* __restrict__ tile_sum) {
+    __shared__ int32_t ws[32];
+    const int q = blockIdx.x * kScanBlock + threadIdx.x;
+    block_inclusive_sum(q < n ? in[q] : 0, ws);
+    if (threadIdx.x == 0) tile_sum[blockIdx.x] = ws[31];
+}
+
+// exclusive scan of the tile totals in place (one block, chunks with a carry); total = sum of all
+__global__ void __launch_bounds__(kScanBlock) k_scan_tile_sums(int32_t* __restrict__ tile_sum, int ntiles,
+                                                               int32_t* __restrict__ total) {
+    __shared__ int32_t ws[32];
+    int32_t carry = 0;
+    for (int base = 0; base < ntiles; base += kScanBlock) {
         const int q = base + threadIdx.x;
-        const int v = q < n ? in[q] : 0;
-        s[threadIdx.x] = v;
-        __syncthreads();
-        for (int off = 1; off < kScanBlock; off <<= 1) {
-            const int t = (int)threadIdx.x >= off ? s[threadIdx.x - off] : 0;
-            __syncthreads();
-            s[threadIdx.x] += t;
-            __syncthreads();
-        }
-        if (q < n) out[q] = carry + s[threadIdx.x] - v;
-        __syncthreads();
-        if (threadIdx.x == kScanBlock - 1) carry += s[threadIdx.x];
+        const int32_t v = q < ntiles ? tile_sum[q] : 0;
+        const int32_t inc = block_inclusive_sum(v, ws);
+        if (q < ntiles) tile_sum[q] = carry + inc - v;
+        carry += ws[31];
         __syncthreads();
     }
     if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_scan_tiles(const int32_t* __restrict__ in, int n,
+                                                           const int32_t* __restrict__ tile_off,
+                                                           int32_t* __restrict__ out) {
+    __shared__ int32_t ws[32];
+    const int q = blockIdx.x * kScanBlock + threadIdx.x;
+    const int32_t v = q < n ? in[q] : 0;
+    const int32_t inc = block_inclusive_sum(v, ws);
+    if (q < n) out[q] = tile_off[blockIdx.x] + inc - v;
 }
 
 // ---------------------------------------------------------------- host driver
@@ -501,9 +535,14 @@ int Ctx::consistency_scan(int mode, int n_views, const int32_t* src_off, const i
             ++launches;
         } else {
             k_fuse_flags<<<blocks, 256, 0, stream>>>(d_views, i, acc, keep, npix);
-            k_exclusive_sum<<<1, kScanBlock, 0, stream>>>(keep, offs, npix, d_total);
-            if (out) k_fuse_emit<<<blocks, 256, 0, stream>>>(d_views, i, keep, offs, out, emitted, capacity, npix);
-            launches += out ? 3 : 2;
+            // block_max is free here (the mark iterations of view i are done): tile totals
+            k_tile_sums<<<nblocks, kScanBlock, 0, stream>>>(keep, npix, block_max);
+            k_scan_tile_sums<<<1, kScanBlock, 0, stream>>>(block_max, nblocks, d_total);
+            if (out) {
+                k_scan_tiles<<<nblocks, kScanBlock, 0, stream>>>(keep, npix, block_max, offs);
+                k_fuse_emit<<<blocks, 256, 0, stream>>>(d_views, i, keep, offs, out, emitted, capacity, npix);
+            }
+            launches += out ? 5 : 3;
             int32_t total = 0;
             e = cudaMemcpyAsync(&total, d_total, 4, cudaMemcpyDeviceToHost, stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(stream);

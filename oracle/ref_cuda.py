@@ -37,6 +37,8 @@ def lib() -> ctypes.CDLL:
         _lib.ref_run_patchmatch.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ora.Params), vp, vp, vp, vp, vp,
                                             vp, vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32,
                                             ctypes.POINTER(ctypes.c_float)]
+        _lib.ref_jbu.restype = ctypes.c_int
+        _lib.ref_jbu.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
         _lib.ref_probe.restype = ctypes.c_int
         _lib.ref_probe.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(ora.Params), vp, vp, vp, ctypes.c_int,
                                    ctypes.c_int, vp, vp, vp, vp, vp, vp]
@@ -94,3 +96,21 @@ def probe(images, depths, cams, params, canny, pix, planes, address_mode: int = 
     out["cost_vec"] = out["cost_vec"][:, :S].copy()
     out["geom"] = out["geom"][:, :S].copy()
     return out
+
+
+def jbu(image, src_depth, src_normal=None):
+    """Raw output of the reference's JBU_cu (src_normal None) or JBU_cu_prior
+    (HPM.cu:3037-3197): the upsampled depth, and for the prior kernel the
+    normalised normals (H x W x 3)."""
+    img = np.ascontiguousarray(image, np.float32)
+    sd = np.ascontiguousarray(src_depth, np.float32)
+    sn = None if src_normal is None else np.ascontiguousarray(src_normal, np.float32)
+    H, W = img.shape
+    sh, sw = sd.shape
+    od = np.zeros((H, W), np.float32)
+    on = None if sn is None else np.zeros((H, W, 3), np.float32)
+    rc = lib().ref_jbu(img.ctypes.data, W, H, sd.ctypes.data, None if sn is None else sn.ctypes.data, sw, sh,
+                       od.ctypes.data, None if on is None else on.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"reference build: JBU probe failed ({rc})")
+    return od if on is None else (od, on)

@@ -10,6 +10,7 @@
 #include "HPM.h"
 #undef private
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -304,5 +305,86 @@ extern "C" int ref_probe(const float* const* images, const float* const* depth_m
         cudaDestroyTextureObject(dh.images[i]);
     }
     for (cudaArray* a : arrs) cudaFreeArray(a);
+    return err == cudaSuccess ? 0 : (int)err;
+}
+
+// ---------------------------------------------------------------------------
+// JBU probes: the reference's own JBU_cu and JBU_cu_prior kernels (HPM.cu:
+// 3037-3197) launched the way JBU::CudaRun does (16x16 blocks), on textures
+// made the way JBUAddImageToTextureFloatGray makes them (HPM.cpp:1213-1239:
+// float, linear filtering, wrap addressing).  Raw kernel output: the host-side
+// NaN fallback of RunJBU (HPM.cpp:1296-1302) is left to the caller.
+__global__ void JBU_cu(JBUParameters* jp, JBUTexObj* jt, float* depth);
+__global__ void JBU_cu_prior(JBUParameters* jp, JBUTexObj* jt, float* depth, float4* normal,
+                             float4* normal_origin_cuda);
+
+// image: W*H grey levels; src_depth: sw*sh; src_normal: sw*sh*3 (prior kernel)
+// or null (plain kernel); out_depth: W*H; out_normal: W*H*3 when src_normal is set.
+extern "C" int ref_jbu(const float* image, int W, int H, const float* src_depth, const float* src_normal, int sw,
+                       int sh, float* out_depth, float* out_normal) {
+    (void)cudaGetLastError();
+    if (W <= 0 || H <= 0 || sw <= 0 || sh <= 0) return -1;
+    const int scale = std::max(H / sh, W / sw);
+    if (scale == 1) return -2;  // RunJBU returns without upsampling (HPM.cpp:1272-1275)
+    JBUParameters jp;
+    jp.height = H;
+    jp.width = W;
+    jp.s_height = sh;
+    jp.s_width = sw;
+    jp.Imagescale = scale;
+    JBUTexObj jt;
+    memset(&jt, 0, sizeof(jt));
+    cudaArray* arrs[2] = {nullptr, nullptr};
+    make_texture(image, W, H, &arrs[0], &jt.imgs[0]);
+    make_texture(src_depth, sw, sh, &arrs[1], &jt.imgs[1]);
+    const size_t n = (size_t)W * H, ns = (size_t)sw * sh;
+    JBUParameters* djp = nullptr;
+    JBUTexObj* djt = nullptr;
+    float* dd = nullptr;
+    float4 *dn = nullptr, *dno = nullptr;
+    cudaMalloc((void**)&djp, sizeof(jp));
+    cudaMalloc((void**)&djt, sizeof(jt));
+    cudaMalloc((void**)&dd, sizeof(float) * n);
+    if (src_normal) {
+        cudaMalloc((void**)&dn, sizeof(float4) * n);
+        cudaMalloc((void**)&dno, sizeof(float4) * ns);
+    }
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) {
+        cudaMemcpy(djp, &jp, sizeof(jp), cudaMemcpyHostToDevice);
+        cudaMemcpy(djt, &jt, sizeof(jt), cudaMemcpyHostToDevice);
+        if (src_normal) {
+            // normal_origin_host: (normal, depth) per coarse pixel (HPM.cpp:1334-1343)
+            std::vector<float4> no(ns);
+            for (size_t i = 0; i < ns; ++i)
+                no[i] = make_float4(src_normal[3 * i], src_normal[3 * i + 1], src_normal[3 * i + 2], src_depth[i]);
+            cudaMemcpy(dno, no.data(), sizeof(float4) * ns, cudaMemcpyHostToDevice);
+        }
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) {
+        const dim3 grid((W + 15) / 16, (H + 15) / 16, 1), block(16, 16, 1);
+        if (src_normal) JBU_cu_prior<<<grid, block>>>(djp, djt, dd, dn, dno);
+        else JBU_cu<<<grid, block>>>(djp, djt, dd);
+        err = cudaDeviceSynchronize();
+    }
+    if (err == cudaSuccess) {
+        err = cudaMemcpy(out_depth, dd, sizeof(float) * n, cudaMemcpyDeviceToHost);
+        if (err == cudaSuccess && src_normal) {
+            std::vector<float4> on(n);
+            err = cudaMemcpy(on.data(), dn, sizeof(float4) * n, cudaMemcpyDeviceToHost);
+            for (size_t i = 0; i < n; ++i) {
+                out_normal[3 * i] = on[i].x;
+                out_normal[3 * i + 1] = on[i].y;
+                out_normal[3 * i + 2] = on[i].z;
+            }
+        }
+    }
+    void* bufs[] = {djp, djt, dd, dn, dno};
+    for (void* b : bufs) cudaFree(b);
+    for (int i = 0; i < 2; ++i) {
+        cudaDestroyTextureObject(jt.imgs[i]);
+        cudaFreeArray(arrs[i]);
+    }
     return err == cudaSuccess ? 0 : (int)err;
 }

@@ -1,11 +1,12 @@
-"""Generates tests/golden/ref_probe.npz: golden vectors of the reference's own
-per-pixel functions (HPM.cu of HPM-MVS++, compiled from its sources by
-oracle/ref_build.mk into oracle/_ref/libhpmref.so) at fixed (pixel, plane)
-pairs of a small seeded synthetic scene.
+"""Generates tests/golden/ref_probe.npz and tests/golden/ref_jbu.npz: golden
+vectors of the reference's own per-pixel functions and JBU kernels (HPM.cu of
+HPM-MVS++, compiled from its sources by oracle/ref_build.mk into
+oracle/_ref/libhpmref.so) on a small seeded synthetic scene.
 
 Needs a CUDA device and the reference build; run from the repository root:
 
     python tests/golden/make_ref_golden.py [--out tests/golden/ref_probe.npz]
+                                           [--jbu-out tests/golden/ref_jbu.npz]
 
 The functions probed (HPM.cu line ranges):
   ComputeMultiViewCostVector                      490-495  per-source bilateral NCC
@@ -13,6 +14,7 @@ The functions probed (HPM.cu line ranges):
   ComputeDepthfromPlaneHypothesis                 154-157
   ComputeGeomConsistencyCost                      539-564  against each source's depth map
   ComputeTexture                                  349-373
+  JBU_cu, JBU_cu_prior (raw kernel output)        3037-3197 upsampling 64x48 -> 128x96
 
 The scene is 5 views of 128x96 (seed 11, 4 sources).  Its grey images are
 integers (stored as uint8) and its depth maps are the ground truth rounded to
@@ -46,6 +48,31 @@ def camera_frame_plane(K, R, n_world, depth, px, py):
     return np.array([n[0], n[1], n[2], -float(n @ X)])
 
 
+def _scene():
+    """The seeded scene and its views, reference first, then its sources in pair order."""
+    from hpm_b200 import synth
+
+    scene = synth.make_scene(n_views=N_VIEWS, width=W, height=H, seed=SEED, n_src=N_VIEWS - 1)
+    order = [0] + [j for j, _ in scene.pairs[0]]
+    return scene, [scene.views[i] for i in order]
+
+
+def make_jbu_inputs() -> dict:
+    """JBU inputs: the reference view's grey image (128x96) and its ground-truth
+    depth (to 1/256) and normals at every second pixel (64x48; the background's
+    zero normals replaced by (0, 0, -1)), one coarse depth set to NaN so the NaN
+    path is exercised."""
+    from hpm_b200 import synth
+
+    _, views = _scene()
+    v0 = views[0]
+    coarse_d = (np.round(v0.depth[::2, ::2].astype(np.float64) * 256.0) / 256.0).astype(np.float32)
+    coarse_d[5, 7] = np.nan
+    coarse_n = np.ascontiguousarray(v0.normal[::2, ::2], np.float32)
+    coarse_n[np.linalg.norm(coarse_n, axis=2) == 0] = (0.0, 0.0, -1.0)  # background: facing the camera
+    return dict(image=synth.gray_float(v0.image).astype(np.uint8), coarse_depth=coarse_d, coarse_normal=coarse_n)
+
+
 def make_inputs() -> dict:
     """Scene, probe pixels and planes: one third ground-truth planes, one third
     perturbed ones (normal noise 0.15, depth within 5 %), the rest random planes
@@ -54,9 +81,7 @@ def make_inputs() -> dict:
     import hpm_b200
     from hpm_b200 import synth
 
-    scene = synth.make_scene(n_views=N_VIEWS, width=W, height=H, seed=SEED, n_src=N_VIEWS - 1)
-    order = [0] + [j for j, _ in scene.pairs[0]]
-    views = [scene.views[i] for i in order]
+    scene, views = _scene()
     grays = np.stack([synth.gray_float(v.image).astype(np.uint8) for v in views])
     depth_q = np.stack([np.round(v.depth.astype(np.float64) * 256.0).astype(np.uint16) for v in views])
     canny = (cv2.Canny(views[0].image, 50, 150) > 0).astype(np.uint8)
@@ -111,6 +136,7 @@ def load(path: str):
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(HERE, "ref_probe.npz"))
+    ap.add_argument("--jbu-out", default=os.path.join(HERE, "ref_jbu.npz"))
     args = ap.parse_args()
     import ref_cuda
 
@@ -126,6 +152,14 @@ def main() -> None:
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     np.savez_compressed(args.out, **inputs, **{"ref_" + k: v for k, v in out.items()})
     print(f"wrote {args.out}: {len(z['pix'])} probes, {len(images) - 1} sources")
+    j = make_jbu_inputs()
+    img = j["image"].astype(np.float32)
+    jbu_depth = ref_cuda.jbu(img, j["coarse_depth"])
+    prior_depth, prior_normal = ref_cuda.jbu(img, j["coarse_depth"], j["coarse_normal"])
+    np.savez_compressed(args.jbu_out, **j, ref_jbu_depth=jbu_depth, ref_jbu_prior_depth=prior_depth,
+                        ref_jbu_prior_normal=prior_normal)
+    print(f"wrote {args.jbu_out}: {img.shape[1]}x{img.shape[0]} from "
+          f"{j['coarse_depth'].shape[1]}x{j['coarse_depth'].shape[0]}")
 
 
 if __name__ == "__main__":

@@ -5,7 +5,9 @@ ComputeMultiViewCostVector, ComputeMultiViewInitialCostandSelectedViews,
 ComputeDepthfromPlaneHypothesis, ComputeGeomConsistencyCost and ComputeTexture
 (the reference compiled from its sources for sm_100a, with its own
 --use_fast_math flags) at 1536 (pixel, plane) pairs of a seeded 5-view scene,
-with the inputs they saw; tests/golden/make_ref_golden.py made it.
+with the inputs they saw; tests/golden/ref_jbu.npz holds the raw output of its
+JBU_cu and JBU_cu_prior kernels upsampling that scene's reference depth and
+normals from 64x48 to 128x96.  tests/golden/make_ref_golden.py made both.
 
 The oracle is IEEE float and evaluates the homography in factored form, so it
 cannot equal fast-math output bit for bit.  What is checked is that every
@@ -40,6 +42,7 @@ import hpm_oracle as ora  # noqa: E402
 import make_ref_golden as golden  # noqa: E402
 
 FIXTURE = os.path.join(HERE, "golden", "ref_probe.npz")
+JBU_FIXTURE = os.path.join(HERE, "golden", "ref_jbu.npz")
 
 U = 2.0 ** -24        # float32 unit roundoff
 TOL_NCC = 2e-4        # per-source bilateral NCC cost, range [0, 2]: 99 % of textured pairs
@@ -49,6 +52,8 @@ MIN_COS = 0.1         # edge-on limit |cos(normal, ray)|
 TOL_DEPTH_REL = 2e-6  # depth of a plane, unless its denominator cancels
 TOL_GEOM = 2e-3       # reprojection distance in pixels, range [0, 3]
 TOL_TEXTURE_REL = 1e-6
+TOL_JBU_REL = 1e-6    # upsampled depth: sums of 25 weighted samples, FMA-contracted in the reference
+TOL_JBU_NORMAL = 1e-6
 
 
 @pytest.fixture(scope="module")
@@ -239,3 +244,47 @@ def test_texture_term_matches_reference(probe):
     ref = z["ref_texture"].astype(np.float64)
     rel = np.abs(got - ref) / np.abs(ref)
     assert rel.max() <= TOL_TEXTURE_REL, rel.max()
+
+
+def jbu_fallback(raw, coarse_depth):
+    """RunJBU's host step (HPM.cpp:1296-1302): a NaN pixel takes the coarse depth at (y/2, x/2)."""
+    out = raw.copy()
+    ys, xs = np.nonzero(np.isnan(raw))
+    out[ys, xs] = coarse_depth[np.minimum(ys // 2, coarse_depth.shape[0] - 1),
+                               np.minimum(xs // 2, coarse_depth.shape[1] - 1)]
+    return out
+
+
+def check_jbu(depth, ref_depth, normal=None, ref_normal=None):
+    """Same NaN positions, finite values within the stated tolerances."""
+    assert np.array_equal(np.isnan(depth), np.isnan(ref_depth))
+    ok = ~np.isnan(ref_depth)
+    rel = np.abs(depth[ok].astype(np.float64) - ref_depth[ok]) / np.maximum(np.abs(ref_depth[ok]), 1e-30)
+    rel[ref_depth[ok] == 0] = np.abs(depth[ok][ref_depth[ok] == 0])
+    assert rel.max() <= TOL_JBU_REL, rel.max()
+    if normal is not None:
+        assert np.array_equal(np.isnan(normal), np.isnan(ref_normal))
+        okn = ~np.isnan(ref_normal)
+        assert np.abs(normal[okn] - ref_normal[okn]).max() <= TOL_JBU_NORMAL
+
+
+@pytest.fixture(scope="module")
+def jbu_probe():
+    assert os.path.exists(JBU_FIXTURE), "tests/golden/ref_jbu.npz is missing (tests/golden/make_ref_golden.py)"
+    return dict(np.load(JBU_FIXTURE))
+
+
+def test_jbu_matches_reference(jbu_probe):
+    j = jbu_probe
+    img = j["image"].astype(np.float32)
+    got = ora.jbu(img, j["coarse_depth"])
+    check_jbu(got, jbu_fallback(j["ref_jbu_depth"], j["coarse_depth"]))
+    assert np.isnan(j["ref_jbu_depth"]).any()  # the NaN path is exercised
+
+
+def test_jbu_prior_matches_reference(jbu_probe):
+    j = jbu_probe
+    img = j["image"].astype(np.float32)
+    d, n = ora.jbu_prior(img, j["coarse_depth"], j["coarse_normal"])
+    # JointBilateralUpsampling_prior keeps the raw output (HPM.cpp:1362-1372)
+    check_jbu(d, j["ref_jbu_prior_depth"], n, j["ref_jbu_prior_normal"])
