@@ -37,12 +37,28 @@ def lib() -> ctypes.CDLL:
         _lib.ref_run_patchmatch.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ora.Params), vp, vp, vp, vp, vp,
                                             vp, vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32,
                                             ctypes.POINTER(ctypes.c_float)]
+        _lib.ref_random_init.restype = ctypes.c_int
+        _lib.ref_random_init.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ora.Params), vp, vp, vp, vp, vp, vp,
+                                         vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32, vp]
         _lib.ref_jbu.restype = ctypes.c_int
         _lib.ref_jbu.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
         _lib.ref_probe.restype = ctypes.c_int
         _lib.ref_probe.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(ora.Params), vp, vp, vp, ctypes.c_int,
                                    ctypes.c_int, vp, vp, vp, vp, vp, vp]
     return _lib
+
+
+def _depth_list(depths, imgs):
+    """One depth map per view, each of its image's size: the driver uploads
+    every entry as a full-size array, so a missing map becomes zeros."""
+    out = []
+    for i, img in enumerate(imgs):
+        d = None if depths is None else depths[i]
+        d = np.zeros(img.shape, np.float32) if d is None else np.ascontiguousarray(d, np.float32)
+        if d.shape != img.shape:
+            raise ValueError(f"depth map {i} has shape {d.shape}, its image {img.shape}")
+        out.append(d)
+    return out
 
 
 def _ptrs(arrs):
@@ -52,8 +68,7 @@ def _ptrs(arrs):
 def run_patchmatch(images, depths, cams, params, st: "ora.RunState", seed: int, view_id: int) -> float:
     """Same arguments and state as hpm_oracle.run_patchmatch; returns the run's device time in ms."""
     imgs = [np.ascontiguousarray(i, np.float32) for i in images]
-    deps = [np.zeros((1, 1), np.float32) if d is None else np.ascontiguousarray(d, np.float32)
-            for d in (depths or [None] * len(imgs))]
+    deps = _depth_list(depths, imgs)
     cam_arr = (ora.Camera * len(cams))(*[ora.to_cam(c) for c in cams])
     prm = ora.to_params(params)
     canny = np.ascontiguousarray(st.canny, np.uint32)
@@ -67,6 +82,26 @@ def run_patchmatch(images, depths, cams, params, st: "ora.RunState", seed: int, 
     if rc != 0:
         raise RuntimeError(f"reference build: CUDA error {rc}")
     return float(ms.value)
+
+
+def random_init(images, depths, cams, params, st: "ora.RunState", seed: int, view_id: int) -> None:
+    """The reference's RandomInitialization kernel alone (HPM.cu:567-763) on the
+    same arguments and state as hpm_oracle.random_init: fills st.planes (camera
+    frame), st.costs, st.selected_views, st.confidences and, outside the prior
+    and mandatory modes, st.texture."""
+    imgs = [np.ascontiguousarray(i, np.float32) for i in images]
+    deps = _depth_list(depths, imgs)
+    cam_arr = (ora.Camera * len(cams))(*[ora.to_cam(c) for c in cams])
+    prm = ora.to_params(params)
+    canny = np.ascontiguousarray(st.canny, np.uint32)
+    scaled = np.ascontiguousarray(st.scaled_planes, np.float32)
+    rc = lib().ref_random_init(_ptrs(imgs), cam_arr, len(imgs), ctypes.byref(prm), st.planes.ctypes.data,
+                               st.costs.ctypes.data, scaled.ctypes.data, st.prior_planes.ctypes.data,
+                               st.plane_masks.ctypes.data, st.confidences.ctypes.data, canny.ctypes.data,
+                               st.texture.ctypes.data, _ptrs(deps), ctypes.c_uint64(seed), view_id,
+                               st.selected_views.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"reference build: RandomInitialization failed ({rc})")
 
 
 def probe(images, depths, cams, params, canny, pix, planes, address_mode: int = 0) -> dict:

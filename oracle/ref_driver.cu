@@ -111,11 +111,21 @@ static void fill_params(PatchMatchParams& p, const RefParams* rp, int num_images
     p.mand_consistency = rp->mode & 32u;
 }
 
-extern "C" int ref_run_patchmatch(const float* const* images, const Camera* cams, int num_images, const RefParams* rp,
-                                  float* planes, float* costs, const float* scaled_planes, const float* prior_planes,
-                                  const unsigned int* plane_masks, float* confidences, const unsigned int* canny,
-                                  float* texture, const float* const* depth_maps, unsigned long long seed,
-                                  unsigned int view, float* elapsed_ms) {
+__global__ void RandomInitialization(cudaTextureObjects* texture_objects, Camera* cameras, float4* plane_hypotheses,
+                                     float4* scaled_plane_hypotheses, float* costs, float* pre_costs,
+                                     curandState* rand_states, unsigned int* selected_views, float4* prior_planes,
+                                     unsigned int* plane_masks, const PatchMatchParams params, float* confidences,
+                                     unsigned int* Canny, float* texture);
+
+// One view's run on an HPM object filled as CudaSpaceInitialization and friends
+// fill it.  init_only: the RandomInitialization kernel alone, launched as
+// RunPatchMatch launches it (HPM.cu:2996-3016), with the planes left in the
+// camera frame and the view masks returned in `selected`.
+static int run_ref(const float* const* images, const Camera* cams, int num_images, const RefParams* rp, float* planes,
+                   float* costs, const float* scaled_planes, const float* prior_planes,
+                   const unsigned int* plane_masks, float* confidences, const unsigned int* canny, float* texture,
+                   const float* const* depth_maps, unsigned long long seed, unsigned int view, float* elapsed_ms,
+                   bool init_only, unsigned int* selected) {
     (void)cudaGetLastError();
     HPM hpm;
     const int W = cams[0].width, H = cams[0].height;
@@ -177,20 +187,58 @@ extern "C" int ref_run_patchmatch(const float* const* images, const Camera* cams
     cudaEventCreate(&b);
     cudaDeviceSynchronize();
     cudaEventRecord(a);
-    hpm.RunPatchMatch();
+    if (init_only) {
+        const dim3 grid((W + 15) / 16, (H + 15) / 16, 1), block(16, 16, 1);
+        RandomInitialization<<<grid, block>>>(hpm.texture_objects_cuda, hpm.cameras_cuda, hpm.plane_hypotheses_cuda,
+                                              hpm.scaled_plane_hypotheses_cuda, hpm.costs_cuda, hpm.pre_costs_cuda,
+                                              hpm.rand_states_cuda, hpm.selected_views_cuda, hpm.prior_planes_cuda,
+                                              hpm.plane_masks_cuda, hpm.params, hpm.confidences_cuda, hpm.Canny_cuda,
+                                              hpm.texture_cuda);
+    } else {
+        hpm.RunPatchMatch();
+    }
     cudaEventRecord(b);
     cudaEventSynchronize(b);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, a, b);
     if (elapsed_ms) *elapsed_ms = ms;
-    memcpy(planes, hpm.plane_hypotheses_host, sizeof(float4) * n);
-    memcpy(costs, hpm.costs_host, sizeof(float) * n);
-    if (!p.mand_consistency && !p.prior_consistency) memcpy(texture, hpm.texture_host, sizeof(float) * n);
+    if (init_only) {
+        cudaMemcpy(planes, hpm.plane_hypotheses_cuda, sizeof(float4) * n, cudaMemcpyDeviceToHost);
+        cudaMemcpy(costs, hpm.costs_cuda, sizeof(float) * n, cudaMemcpyDeviceToHost);
+        cudaMemcpy(selected, hpm.selected_views_cuda, sizeof(unsigned int) * n, cudaMemcpyDeviceToHost);
+        if (!p.mand_consistency && !p.prior_consistency)
+            cudaMemcpy(texture, hpm.texture_cuda, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    } else {
+        memcpy(planes, hpm.plane_hypotheses_host, sizeof(float4) * n);
+        memcpy(costs, hpm.costs_host, sizeof(float) * n);
+        if (!p.mand_consistency && !p.prior_consistency) memcpy(texture, hpm.texture_host, sizeof(float) * n);
+    }
     cudaMemcpy(confidences, hpm.confidences_cuda, sizeof(float) * n, cudaMemcpyDeviceToHost);
     const cudaError_t err = cudaDeviceSynchronize();
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     return err == cudaSuccess ? 0 : (int)err;
+}
+
+extern "C" int ref_run_patchmatch(const float* const* images, const Camera* cams, int num_images, const RefParams* rp,
+                                  float* planes, float* costs, const float* scaled_planes, const float* prior_planes,
+                                  const unsigned int* plane_masks, float* confidences, const unsigned int* canny,
+                                  float* texture, const float* const* depth_maps, unsigned long long seed,
+                                  unsigned int view, float* elapsed_ms) {
+    return run_ref(images, cams, num_images, rp, planes, costs, scaled_planes, prior_planes, plane_masks, confidences,
+                   canny, texture, depth_maps, seed, view, elapsed_ms, false, nullptr);
+}
+
+// The reference's RandomInitialization alone (HPM.cu:567-763): same arguments
+// as ref_run_patchmatch plus the per-pixel view masks it writes.
+extern "C" int ref_random_init(const float* const* images, const Camera* cams, int num_images, const RefParams* rp,
+                               float* planes, float* costs, const float* scaled_planes, const float* prior_planes,
+                               const unsigned int* plane_masks, float* confidences, const unsigned int* canny,
+                               float* texture, const float* const* depth_maps, unsigned long long seed,
+                               unsigned int view, unsigned int* selected) {
+    if (!selected) return -1;
+    return run_ref(images, cams, num_images, rp, planes, costs, scaled_planes, prior_planes, plane_masks, confidences,
+                   canny, texture, depth_maps, seed, view, nullptr, true, selected);
 }
 
 // ---------------------------------------------------------------------------

@@ -7,7 +7,10 @@ ComputeDepthfromPlaneHypothesis, ComputeGeomConsistencyCost and ComputeTexture
 --use_fast_math flags) at 1536 (pixel, plane) pairs of a seeded 5-view scene,
 with the inputs they saw; tests/golden/ref_jbu.npz holds the raw output of its
 JBU_cu and JBU_cu_prior kernels upsampling that scene's reference depth and
-normals from 64x48 to 128x96.  tests/golden/make_ref_golden.py made both.
+normals from 64x48 to 128x96; tests/golden/ref_init.npz holds the output of its
+RandomInitialization kernel in the photometric, geometric, mandatory, prior
+and hierarchy modes on a 64x48 view, its random draws routed to the shared
+Philox stream.  tests/golden/make_ref_golden.py made all three.
 
 The oracle is IEEE float and evaluates the homography in factored form, so it
 cannot equal fast-math output bit for bit.  What is checked is that every
@@ -15,7 +18,9 @@ difference is of the size float32 rounding explains:
 
 - on textured patches, costs agree to 2e-4 at 99 % of (probe, source) pairs
   and to 1.5e-3 everywhere (a sample position that moves by a few ulps can
-  cross one of the texture unit's 1/256 weight steps);
+  cross one of the texture unit's 1/256 weight steps); for oblique planes the
+  patch is stretched along the tilt and that bound grows as 0.45 / |cos|,
+  |cos| between the normal and the pixel's ray;
 - on patches of pure noise (the scene's background: grey about 190, sigma 2)
   the reference's variance E[x^2] - E[x]^2 cancels catastrophically, and the
   difference stays within 16 unit roundoffs of the magnitudes that cancel
@@ -43,17 +48,20 @@ import make_ref_golden as golden  # noqa: E402
 
 FIXTURE = os.path.join(HERE, "golden", "ref_probe.npz")
 JBU_FIXTURE = os.path.join(HERE, "golden", "ref_jbu.npz")
+INIT_FIXTURE = os.path.join(HERE, "golden", "ref_init.npz")
 
 U = 2.0 ** -24        # float32 unit roundoff
 TOL_NCC = 2e-4        # per-source bilateral NCC cost, range [0, 2]: 99 % of textured pairs
 TOL_NCC_MAX = 1.5e-3  # every pair that is not edge-on, unless the rounding scale allows more
 K_NCC = 16            # unit roundoffs of the cancelling magnitudes
 MIN_COS = 0.1         # edge-on limit |cos(normal, ray)|
+COS_FULL = 0.45       # below this |cos| the position bound scales as COS_FULL / |cos|
 TOL_DEPTH_REL = 2e-6  # depth of a plane, unless its denominator cancels
 TOL_GEOM = 2e-3       # reprojection distance in pixels, range [0, 3]
 TOL_TEXTURE_REL = 1e-6
 TOL_JBU_REL = 1e-6    # upsampled depth: sums of 25 weighted samples, FMA-contracted in the reference
 TOL_JBU_NORMAL = 1e-6
+TOL_INIT_NORMAL = 1e-6  # generated and transformed normals, per component
 
 
 @pytest.fixture(scope="module")
@@ -131,20 +139,31 @@ def ncc_rounding_scale(images, cams, params, pix, planes) -> np.ndarray:
     return out
 
 
-def edge_on(cams, pix, planes) -> np.ndarray:
-    """|cos| between the plane normal and the pixel's viewing ray below MIN_COS."""
+def view_cos(cams, pix, planes) -> np.ndarray:
+    """|cos| between the plane normal and the pixel's viewing ray."""
     K = _mat(cams[0], "K", (3, 3))
     ray = np.stack([(pix[:, 0] - K[0, 2]) / K[0, 0], (pix[:, 1] - K[1, 2]) / K[1, 1], np.ones(len(pix))], 1)
     n = planes[:, :3].astype(np.float64)
-    cos = np.abs((n * ray).sum(1)) / (np.linalg.norm(n, axis=1) * np.linalg.norm(ray, axis=1))
-    return cos < MIN_COS
+    return np.abs((n * ray).sum(1)) / (np.linalg.norm(n, axis=1) * np.linalg.norm(ray, axis=1))
+
+
+def edge_on(cams, pix, planes) -> np.ndarray:
+    return view_cos(cams, pix, planes) < MIN_COS
+
+
+def cost_allowance(images, cams, params, pix, planes) -> np.ndarray:
+    """Allowed |difference| per (probe, source): the larger of the position
+    bound (TOL_NCC_MAX, scaled by COS_FULL / |cos| for oblique planes) and
+    K_NCC unit roundoffs of the cancelling magnitudes."""
+    cos = np.maximum(view_cos(cams, pix, planes), MIN_COS)
+    floor = TOL_NCC_MAX * np.maximum(1.0, COS_FULL / cos)
+    return np.maximum(floor[:, None], K_NCC * ncc_rounding_scale(images, cams, params, pix, planes))
 
 
 def ncc_allowance(images, depths, cams, params, z):
     """(allowed |difference| per (probe, source), textured mask, edge-on mask)."""
-    scale = ncc_rounding_scale(images, cams, params, z["pix"], z["planes"])
-    allow = np.maximum(TOL_NCC_MAX, K_NCC * scale)
-    textured = (depths[0][z["pix"][:, 1], z["pix"][:, 0]] > 0)[:, None] & np.ones((1, scale.shape[1]), bool)
+    allow = cost_allowance(images, cams, params, z["pix"], z["planes"])
+    textured = (depths[0][z["pix"][:, 1], z["pix"][:, 0]] > 0)[:, None] & np.ones((1, allow.shape[1]), bool)
     return allow, textured, edge_on(cams, z["pix"], z["planes"])
 
 
@@ -288,3 +307,48 @@ def test_jbu_prior_matches_reference(jbu_probe):
     d, n = ora.jbu_prior(img, j["coarse_depth"], j["coarse_normal"])
     # JointBilateralUpsampling_prior keeps the raw output (HPM.cpp:1362-1372)
     check_jbu(d, j["ref_jbu_prior_depth"], n, j["ref_jbu_prior_normal"])
+
+
+@pytest.fixture(scope="module")
+def init_probe():
+    assert os.path.exists(INIT_FIXTURE), "tests/golden/ref_init.npz is missing (tests/golden/make_ref_golden.py)"
+    return dict(np.load(INIT_FIXTURE))
+
+
+@pytest.mark.parametrize("name,mode", golden.INIT_CASES, ids=[c[0] for c in golden.INIT_CASES])
+def test_random_init_matches_reference(init_probe, name, mode):
+    """RandomInitialization (HPM.cu:567-763) per pixel: the generated or
+    reloaded plane, its initial cost and view mask, the texture term and the
+    mandatory mode's confidence update."""
+    z = init_probe
+    images, _, cams, params, st = golden.init_state(z, mode)
+    ora.random_init(images, cams, params, st, golden.INIT_RUN_SEED, 0)
+    rp = z[f"ref_{name}_planes"]
+    assert np.abs(st.planes[..., :3] - rp[..., :3]).max() <= TOL_INIT_NORMAL
+    # plane offset w = -n.X: within 32 roundoffs of the magnitudes of its terms
+    K = _mat(cams[0], "K", (3, 3))
+    H, W = rp.shape[:2]
+    ys, xs = np.mgrid[0:H, 0:W].astype(np.float64)
+    n = rp[..., :3].astype(np.float64)
+    w = rp[..., 3].astype(np.float64)
+    den = (xs - K[0, 2]) * n[..., 0] + K[0, 0] / K[1, 1] * (ys - K[1, 2]) * n[..., 1] + K[0, 0] * n[..., 2]
+    depth = -w * K[0, 0] / den
+    X = np.stack([depth * (xs - K[0, 2]) / K[0, 0], depth * (ys - K[1, 2]) / K[1, 1], depth], axis=-1)
+    terms = np.abs(n * X).sum(axis=-1)
+    dw = np.abs(st.planes[..., 3].astype(np.float64) - w)
+    assert (dw <= np.maximum(1e-6 * np.abs(w), 32 * U * terms)).all()
+    assert np.array_equal(st.selected_views, z[f"ref_{name}_selected"])
+    # costs: the NCC criteria of the per-function vectors, at the reference's planes
+    pix = np.stack([xs.ravel(), ys.ravel()], axis=1).astype(np.int32)
+    planes = rp.reshape(-1, 4)
+    allow = cost_allowance(images, cams, params, pix, planes).max(axis=1)
+    edge = edge_on(cams, pix, planes)
+    d = np.abs(st.costs - z[f"ref_{name}_costs"]).ravel()
+    bad = ~edge & (d > allow)
+    assert not bad.any(), [(int(k), float(d[k]), float(allow[k])) for k in np.nonzero(bad)[0][:5]]
+    assert np.median(d[~edge]) <= 2e-5 and (d[~edge] <= TOL_NCC).mean() >= 0.8
+    if f"ref_{name}_texture" in z:
+        t = z[f"ref_{name}_texture"]
+        assert (np.abs(st.texture - t) <= TOL_TEXTURE_REL * np.abs(t)).all()
+    if f"ref_{name}_confidences" in z:
+        assert np.array_equal(st.confidences, z[f"ref_{name}_confidences"])
