@@ -734,12 +734,15 @@ __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const 
                         }
                     }
                 }
-                // plane_hypotheses_now is uninitialised in the reference (HPM.cu:1844, 2299); it
-                // starts as the pixel's current plane here.
+                // plane_hypotheses_now (HPM.cu:1843, 2298) is assigned only when the neighbour
+                // is accepted; the reference as compiled holds the minimum-cost neighbour's plane
+                // whenever that direction is valid.  Otherwise (and in prior mode) it starts as
+                // the pixel's current plane.
                 plane_now = cur;
                 if ((MAND || !prior) && min_valid) {
                     const float4 pd = a.planes[s.pos(min_idx)];
                     const float db = depth_from_plane(c0, pd, px, py);
+                    plane_now = pd;
                     if (db >= dmin && db <= dmax && fcl[min_idx] < cost_now) {
                         depth_now = db; plane_now = pd; cost_now = fcl[min_idx];
                         a.sel[center] = sel.temp_selected;
@@ -795,10 +798,11 @@ __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const 
                 const float rnow = (cc > 0) ? fmaxf(3.0f, mce) * gce : mce * gce;
                 if (cc < 0.3) cost_u = (float)(cost_u * exp(0.2 + cc * 2));
                 else cost_u = cost_u * hpm_expf(-cc * 2);
-                float4 pu = cur;  // uninitialised in the reference (HPM.cu:2761)
+                float4 pu = cur;  // HPM.cu:2760: the neighbour's plane whenever that direction is valid
                 if (flags & (1u << max_idx)) {
                     const int pm = s.pos(max_idx);
                     const float4 pd = a.planes[pm];
+                    pu = pd;
                     const float db = depth_from_plane(c0, pd, px, py);
                     if (db >= dmin && db <= dmax && rfc[max_idx] > rnow) {
                         pu = pd; cost_u = fcl[max_idx];

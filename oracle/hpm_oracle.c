@@ -934,10 +934,16 @@ static void propagate_pixel(const float *const *images, const float *const *dept
         }
     }
 
-    f4 plane_now = load4(st->planes, center); /* defined value for the uninitialised local (HPM.cu:1844) */
+    /* plane_hypotheses_now (HPM.cu:1843) is assigned only when the neighbour is
+     * accepted.  The reference as compiled holds the minimum-cost neighbour's
+     * plane in it whenever that direction is valid, accepted or not (its
+     * half-sweep golden vectors, tests/golden/ref_init.npz); elsewhere -- an
+     * invalid direction, and prior mode -- it starts as the pixel's current plane. */
+    f4 plane_now = load4(st->planes, center);
     if (!prior && s.flag[min_idx]) {
         const f4 pl = load4(st->planes, s.positions[min_idx]);
         const float db = depth_from_plane(c0, pl, px, py);
+        plane_now = pl;
         if (db >= prm->depth_min && db <= prm->depth_max && s.final_costs[min_idx] < cost_now) {
             depth_now = db; plane_now = pl; cost_now = s.final_costs[min_idx];
             st->selected_views[center] = s.temp_selected;
@@ -979,10 +985,11 @@ static void propagate_pixel_mand(const float *const *images, const float *const 
                                       s.view_weights, s.weight_norm);
         st->costs[center] = cost_now;
         float depth_now = depth_from_plane(c0, load4(st->planes, center), px, py);
-        f4 plane_now = load4(st->planes, center);
+        f4 plane_now = load4(st->planes, center); /* HPM.cu:2298: read as at HPM.cu:1843 */
         if (s.flag[min_idx]) {
             const f4 pl = load4(st->planes, s.positions[min_idx]);
             const float db = depth_from_plane(c0, pl, px, py);
+            plane_now = pl;
             if (db >= prm->depth_min && db <= prm->depth_max && s.final_costs[min_idx] < cost_now) {
                 depth_now = db; plane_now = pl; cost_now = s.final_costs[min_idx];
                 st->selected_views[center] = s.temp_selected;
@@ -1030,10 +1037,13 @@ static void propagate_pixel_mand(const float *const *images, const float *const 
     if (cc < 0.3) cost_now = (float)(cost_now * exp(0.2 + cc * 2));
     else cost_now = cost_now * hpm_expf(-cc * 2);
 
-    f4 plane_now = load4(st->planes, center); /* defined value for HPM.cu:2761 */
+    /* HPM.cu:2760: the maximum-score neighbour's plane whenever that direction
+     * is valid, as at HPM.cu:1843; the pixel's current plane otherwise */
+    f4 plane_now = load4(st->planes, center);
     if (s.flag[max_idx]) {
         const int pm = s.positions[max_idx];
         const f4 pl = load4(st->planes, pm);
+        plane_now = pl;
         const float db = depth_from_plane(c0, pl, px, py);
         if (db >= prm->depth_min && db <= prm->depth_max && rfc[max_idx] > rnow) {
             plane_now = pl; cost_now = s.final_costs[max_idx];

@@ -39,7 +39,7 @@ def lib() -> ctypes.CDLL:
                                             ctypes.POINTER(ctypes.c_float)]
         _lib.ref_random_init.restype = ctypes.c_int
         _lib.ref_random_init.argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(ora.Params), vp, vp, vp, vp, vp, vp,
-                                         vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32, vp]
+                                         vp, vp, vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, vp]
         _lib.ref_jbu.restype = ctypes.c_int
         _lib.ref_jbu.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
         _lib.ref_probe.restype = ctypes.c_int
@@ -84,8 +84,10 @@ def run_patchmatch(images, depths, cams, params, st: "ora.RunState", seed: int, 
     return float(ms.value)
 
 
-def random_init(images, depths, cams, params, st: "ora.RunState", seed: int, view_id: int) -> None:
-    """The reference's RandomInitialization kernel alone (HPM.cu:567-763) on the
+def random_init(images, depths, cams, params, st: "ora.RunState", seed: int, view_id: int,
+                n_half: int = 0) -> None:
+    """The reference's RandomInitialization kernel (HPM.cu:567-763), followed by
+    its first n_half half-sweeps (Black, Red, ...; HPM.cu:2793-2827), on the
     same arguments and state as hpm_oracle.random_init: fills st.planes (camera
     frame), st.costs, st.selected_views, st.confidences and, outside the prior
     and mandatory modes, st.texture."""
@@ -98,7 +100,7 @@ def random_init(images, depths, cams, params, st: "ora.RunState", seed: int, vie
     rc = lib().ref_random_init(_ptrs(imgs), cam_arr, len(imgs), ctypes.byref(prm), st.planes.ctypes.data,
                                st.costs.ctypes.data, scaled.ctypes.data, st.prior_planes.ctypes.data,
                                st.plane_masks.ctypes.data, st.confidences.ctypes.data, canny.ctypes.data,
-                               st.texture.ctypes.data, _ptrs(deps), ctypes.c_uint64(seed), view_id,
+                               st.texture.ctypes.data, _ptrs(deps), ctypes.c_uint64(seed), view_id, n_half,
                                st.selected_views.ctypes.data)
     if rc != 0:
         raise RuntimeError(f"reference build: RandomInitialization failed ({rc})")

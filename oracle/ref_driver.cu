@@ -117,15 +117,29 @@ __global__ void RandomInitialization(cudaTextureObjects* texture_objects, Camera
                                      unsigned int* plane_masks, const PatchMatchParams params, float* confidences,
                                      unsigned int* Canny, float* texture);
 
+__global__ void BlackPixelUpdate(cudaTextureObjects* texture_objects, cudaTextureObjects* texture_depths,
+                                 Camera* cameras, float4* plane_hypotheses, float* costs, float* pre_costs,
+                                 curandState* rand_states, unsigned int* selected_views, float4* prior_planes,
+                                 unsigned int* plane_masks, const PatchMatchParams params, const int iter,
+                                 float* confidences, unsigned int* Canny);
+__global__ void RedPixelUpdate(cudaTextureObjects* texture_objects, cudaTextureObjects* texture_depths,
+                               Camera* cameras, float4* plane_hypotheses, float* costs, float* pre_costs,
+                               curandState* rand_states, unsigned int* selected_views, float4* prior_planes,
+                               unsigned int* plane_masks, const PatchMatchParams params, const int iter,
+                               float* confidences, unsigned int* Canny);
+
 // One view's run on an HPM object filled as CudaSpaceInitialization and friends
-// fill it.  init_only: the RandomInitialization kernel alone, launched as
-// RunPatchMatch launches it (HPM.cu:2996-3016), with the planes left in the
-// camera frame and the view masks returned in `selected`.
+// fill it.  n_half < 0: HPM::RunPatchMatch unchanged.  n_half >= 0: the
+// RandomInitialization kernel followed by the first n_half half-sweeps
+// (Black, Red, Black, ...), launched as RunPatchMatch launches them
+// (HPM.cu:2987-3021), with the planes left in the camera frame and the view
+// masks returned in `selected`.
 static int run_ref(const float* const* images, const Camera* cams, int num_images, const RefParams* rp, float* planes,
                    float* costs, const float* scaled_planes, const float* prior_planes,
                    const unsigned int* plane_masks, float* confidences, const unsigned int* canny, float* texture,
                    const float* const* depth_maps, unsigned long long seed, unsigned int view, float* elapsed_ms,
-                   bool init_only, unsigned int* selected) {
+                   int n_half, unsigned int* selected) {
+    const bool init_only = n_half >= 0;
     (void)cudaGetLastError();
     HPM hpm;
     const int W = cams[0].width, H = cams[0].height;
@@ -194,6 +208,22 @@ static int run_ref(const float* const* images, const Camera* cams, int num_image
                                               hpm.rand_states_cuda, hpm.selected_views_cuda, hpm.prior_planes_cuda,
                                               hpm.plane_masks_cuda, hpm.params, hpm.confidences_cuda, hpm.Canny_cuda,
                                               hpm.texture_cuda);
+        const dim3 cgrid((W + 31) / 32, ((H / 2) + 15) / 16, 1), cblock(32, 16, 1);
+        for (int h = 0; h < n_half; ++h) {
+            if (h % 2 == 0)
+                BlackPixelUpdate<<<cgrid, cblock>>>(hpm.texture_objects_cuda, hpm.texture_depths_cuda,
+                                                    hpm.cameras_cuda, hpm.plane_hypotheses_cuda, hpm.costs_cuda,
+                                                    hpm.pre_costs_cuda, hpm.rand_states_cuda,
+                                                    hpm.selected_views_cuda, hpm.prior_planes_cuda,
+                                                    hpm.plane_masks_cuda, hpm.params, h / 2, hpm.confidences_cuda,
+                                                    hpm.Canny_cuda);
+            else
+                RedPixelUpdate<<<cgrid, cblock>>>(hpm.texture_objects_cuda, hpm.texture_depths_cuda,
+                                                  hpm.cameras_cuda, hpm.plane_hypotheses_cuda, hpm.costs_cuda,
+                                                  hpm.pre_costs_cuda, hpm.rand_states_cuda, hpm.selected_views_cuda,
+                                                  hpm.prior_planes_cuda, hpm.plane_masks_cuda, hpm.params, h / 2,
+                                                  hpm.confidences_cuda, hpm.Canny_cuda);
+        }
     } else {
         hpm.RunPatchMatch();
     }
@@ -226,19 +256,20 @@ extern "C" int ref_run_patchmatch(const float* const* images, const Camera* cams
                                   float* texture, const float* const* depth_maps, unsigned long long seed,
                                   unsigned int view, float* elapsed_ms) {
     return run_ref(images, cams, num_images, rp, planes, costs, scaled_planes, prior_planes, plane_masks, confidences,
-                   canny, texture, depth_maps, seed, view, elapsed_ms, false, nullptr);
+                   canny, texture, depth_maps, seed, view, elapsed_ms, -1, nullptr);
 }
 
-// The reference's RandomInitialization alone (HPM.cu:567-763): same arguments
-// as ref_run_patchmatch plus the per-pixel view masks it writes.
+// The reference's RandomInitialization (HPM.cu:567-763) and its first n_half
+// half-sweeps (HPM.cu:2793-2827): same arguments as ref_run_patchmatch plus
+// the per-pixel view masks.
 extern "C" int ref_random_init(const float* const* images, const Camera* cams, int num_images, const RefParams* rp,
                                float* planes, float* costs, const float* scaled_planes, const float* prior_planes,
                                const unsigned int* plane_masks, float* confidences, const unsigned int* canny,
                                float* texture, const float* const* depth_maps, unsigned long long seed,
-                               unsigned int view, unsigned int* selected) {
-    if (!selected) return -1;
+                               unsigned int view, int n_half, unsigned int* selected) {
+    if (!selected || n_half < 0 || n_half > 6) return -1;
     return run_ref(images, cams, num_images, rp, planes, costs, scaled_planes, prior_planes, plane_masks, confidences,
-                   canny, texture, depth_maps, seed, view, nullptr, true, selected);
+                   canny, texture, depth_maps, seed, view, nullptr, n_half, selected);
 }
 
 // ---------------------------------------------------------------------------
