@@ -693,6 +693,8 @@ __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const 
                 depth_now = depth_from_plane(c0, cur, px, py);
                 restricted_cost = 0.0f;
                 texture = 0.0f;
+                float4 prior_pick = cur;  // prior mode: the maximum-score neighbour's plane, when valid
+                bool has_pick = false;
                 if (!MAND && prior) {
                     pp = a.prior[center];
                     depth_prior = depth_from_plane(c0, pp, px, py);
@@ -714,6 +716,8 @@ __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const 
                         if (flags & (1u << max_idx)) {
                             const float4 pd = a.planes[s.pos(max_idx)];
                             const float db = depth_from_plane(c0, pd, px, py);
+                            prior_pick = pd;
+                            has_pick = true;
                             if (db >= dmin && db <= dmax && rfc[max_idx] > rnow) {
                                 depth_now = db;
                                 cur = pd;
@@ -736,9 +740,10 @@ __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const 
                 }
                 // plane_hypotheses_now (HPM.cu:1843, 2298) is assigned only when the neighbour
                 // is accepted; the reference as compiled holds the minimum-cost neighbour's plane
-                // whenever that direction is valid.  Otherwise (and in prior mode) it starts as
-                // the pixel's current plane.
-                plane_now = cur;
+                // whenever that direction is valid; prior mode never assigns it and holds the
+                // maximum-score neighbour's plane when valid.  Otherwise it starts as the
+                // pixel's current plane.
+                plane_now = (!MAND && prior && has_pick) ? prior_pick : cur;
                 if ((MAND || !prior) && min_valid) {
                     const float4 pd = a.planes[s.pos(min_idx)];
                     const float db = depth_from_plane(c0, pd, px, py);

@@ -892,6 +892,8 @@ static void propagate_pixel(const float *const *images, const float *const *dept
     float depth_now = depth_from_plane(c0, load4(st->planes, center), px, py);
     float restricted_cost = 0.0f;
     float texture = 0.0f;
+    f4 prior_pick = load4(st->planes, center);
+    int has_pick = 0;
     if (prior) {
         const float depth_sigma = (prm->depth_max - prm->depth_min) / 64.0f;
         const float two_dss = 2 * depth_sigma * depth_sigma;
@@ -915,6 +917,8 @@ static void propagate_pixel(const float *const *images, const float *const *dept
             if (s.flag[max_idx]) {
                 const f4 pl = load4(st->planes, s.positions[max_idx]);
                 const float db = depth_from_plane(c0, pl, px, py);
+                prior_pick = pl;
+                has_pick = 1;
                 if (db >= prm->depth_min && db <= prm->depth_max && rfc[max_idx] > rnow) {
                     depth_now = db;
                     store4(st->planes, center, pl);
@@ -937,9 +941,12 @@ static void propagate_pixel(const float *const *images, const float *const *dept
     /* plane_hypotheses_now (HPM.cu:1843) is assigned only when the neighbour is
      * accepted.  The reference as compiled holds the minimum-cost neighbour's
      * plane in it whenever that direction is valid, accepted or not (its
-     * half-sweep golden vectors, tests/golden/ref_init.npz); elsewhere -- an
-     * invalid direction, and prior mode -- it starts as the pixel's current plane. */
+     * half-sweep golden vectors, tests/golden/ref_init.npz).  Prior mode never
+     * assigns it; there the compiled reference holds the maximum-score
+     * neighbour's plane when that direction is valid.  Elsewhere (an invalid
+     * direction) it starts as the pixel's current plane. */
     f4 plane_now = load4(st->planes, center);
+    if (prior && has_pick) plane_now = prior_pick;
     if (!prior && s.flag[min_idx]) {
         const f4 pl = load4(st->planes, s.positions[min_idx]);
         const float db = depth_from_plane(c0, pl, px, py);

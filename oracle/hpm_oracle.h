@@ -26,8 +26,9 @@
  * Where the reference reads uninitialised memory this oracle and the CUDA path
  * use the same defined value:
  *  - plane_hypotheses_now (HPM.cu:1843, 2298, 2760) holds the best valid
- *    neighbour's plane (as the compiled reference does), else -- and always in
- *    prior mode -- the pixel's current plane;
+ *    neighbour's plane (minimum cost; maximum score in prior mode and for
+ *    unreliable mandatory pixels), as the compiled reference does, else the
+ *    pixel's current plane;
  *  - the hierarchy pre-cost plane (HPM.cpp:894-901 leaves xyz unset) has a zero
  *    normal;
  *  - selected_views starts at zero at every run (fresh cudaMalloc, HPM.cpp:782).
