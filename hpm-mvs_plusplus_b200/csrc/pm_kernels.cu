@@ -719,7 +719,8 @@ __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const 
                             prior_pick = pd;
                             has_pick = true;
                             if (db >= dmin && db <= dmax && rfc[max_idx] > rnow) {
-                                depth_now = db;
+                                // depth_now is left alone: HPM.cu:1815 shadows it in this block, so
+                                // the refinement receives the pre-acceptance depth
                                 cur = pd;
                                 a.planes[center] = pd;
                                 a.costs[center] = fcl[max_idx];
@@ -738,7 +739,7 @@ __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const 
                         }
                     }
                 }
-                // plane_hypotheses_now (HPM.cu:1843, 2298) is assigned only when the neighbour
+                // plane_hypotheses_now (HPM.cu:1844, 2299) is assigned only when the neighbour
                 // is accepted; the reference as compiled holds the minimum-cost neighbour's plane
                 // whenever that direction is valid; prior mode never assigns it and holds the
                 // maximum-score neighbour's plane when valid.  Otherwise it starts as the
@@ -803,7 +804,7 @@ __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const 
                 const float rnow = (cc > 0) ? fmaxf(3.0f, mce) * gce : mce * gce;
                 if (cc < 0.3) cost_u = (float)(cost_u * exp(0.2 + cc * 2));
                 else cost_u = cost_u * hpm_expf(-cc * 2);
-                float4 pu = cur;  // HPM.cu:2760: the neighbour's plane whenever that direction is valid
+                float4 pu = cur;  // HPM.cu:2761: the neighbour's plane whenever that direction is valid
                 if (flags & (1u << max_idx)) {
                     const int pm = s.pos(max_idx);
                     const float4 pd = a.planes[pm];

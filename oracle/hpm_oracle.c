@@ -920,7 +920,9 @@ static void propagate_pixel(const float *const *images, const float *const *dept
                 prior_pick = pl;
                 has_pick = 1;
                 if (db >= prm->depth_min && db <= prm->depth_max && rfc[max_idx] > rnow) {
-                    depth_now = db;
+                    /* no depth_now = db: HPM.cu:1815 declares a second depth_now in this
+                     * block, so the assignment at HPM.cu:1825 never reaches the depth the
+                     * refinement receives (the pre-acceptance depth) */
                     store4(st->planes, center, pl);
                     st->costs[center] = s.final_costs[max_idx];
                     restricted_cost = rfc[max_idx];
@@ -938,7 +940,7 @@ static void propagate_pixel(const float *const *images, const float *const *dept
         }
     }
 
-    /* plane_hypotheses_now (HPM.cu:1843) is assigned only when the neighbour is
+    /* plane_hypotheses_now (HPM.cu:1844) is assigned only when the neighbour is
      * accepted.  The reference as compiled holds the minimum-cost neighbour's
      * plane in it whenever that direction is valid, accepted or not (its
      * half-sweep golden vectors, tests/golden/ref_init.npz).  Prior mode never
@@ -992,7 +994,7 @@ static void propagate_pixel_mand(const float *const *images, const float *const 
                                       s.view_weights, s.weight_norm);
         st->costs[center] = cost_now;
         float depth_now = depth_from_plane(c0, load4(st->planes, center), px, py);
-        f4 plane_now = load4(st->planes, center); /* HPM.cu:2298: read as at HPM.cu:1843 */
+        f4 plane_now = load4(st->planes, center); /* HPM.cu:2299: read as at HPM.cu:1844 */
         if (s.flag[min_idx]) {
             const f4 pl = load4(st->planes, s.positions[min_idx]);
             const float db = depth_from_plane(c0, pl, px, py);
@@ -1044,8 +1046,8 @@ static void propagate_pixel_mand(const float *const *images, const float *const 
     if (cc < 0.3) cost_now = (float)(cost_now * exp(0.2 + cc * 2));
     else cost_now = cost_now * hpm_expf(-cc * 2);
 
-    /* HPM.cu:2760: the maximum-score neighbour's plane whenever that direction
-     * is valid, as at HPM.cu:1843; the pixel's current plane otherwise */
+    /* HPM.cu:2761: the maximum-score neighbour's plane whenever that direction
+     * is valid, as at HPM.cu:1844; the pixel's current plane otherwise */
     f4 plane_now = load4(st->planes, center);
     if (s.flag[max_idx]) {
         const int pm = s.positions[max_idx];

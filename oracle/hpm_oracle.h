@@ -25,7 +25,7 @@
  *
  * Where the reference reads uninitialised memory this oracle and the CUDA path
  * use the same defined value:
- *  - plane_hypotheses_now (HPM.cu:1843, 2298, 2760) holds the best valid
+ *  - plane_hypotheses_now (HPM.cu:1844, 2299, 2761) holds the best valid
  *    neighbour's plane (minimum cost; maximum score in prior mode and for
  *    unreliable mandatory pixels), as the compiled reference does, else the
  *    pixel's current plane;

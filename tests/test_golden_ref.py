@@ -356,23 +356,29 @@ def test_random_init_matches_reference(init_probe, name, mode):
 
 
 # Share of updated pixels whose plane after the half-sweeps equals the
-# reference's, away from the 6-pixel border band.  Inside the band the
-# reference reads an unassigned plane_hypotheses_now (HPM.cu:1843) whenever its
-# minimum-cost direction lies outside the image, and prior mode reads it at
-# every pixel; what the compiled code holds there is not a value of the
+# reference's, starting from the reference's own initial state, away from the
+# 6-pixel border band.  The rest of the interior are candidates whose costs tie
+# within rounding.  Inside the band the reference reads an unassigned
+# plane_hypotheses_now (HPM.cu:1844) whenever its minimum-cost direction lies
+# outside the image; what the compiled code holds there is not a value of the
 # algorithm, so those pixels are measured, not required.
-SWEEP_MIN_SAME = {("photometric", 1): 0.95, ("photometric", 2): 0.87, ("geometric", 1): 0.97,
-                  ("mandatory", 1): 0.97, ("prior", 1): 0.78}
+SWEEP_MIN_SAME = {("photometric", 1): 0.97, ("photometric", 2): 0.92, ("geometric", 1): 0.97,
+                  ("mandatory", 1): 0.97, ("prior", 1): 0.99}
 
 
 @pytest.mark.parametrize("name,mode,n_half", golden.SWEEP_CASES, ids=[f"{c[0]}-h{c[2]}" for c in golden.SWEEP_CASES])
 def test_half_sweeps_match_reference(init_probe, name, mode, n_half):
     """CheckerboardPropagation and its refinement (HPM.cu:765-1873, 1875-2791):
-    a half-sweep reads only the other colour, so it is deterministic, and from
-    the same initial state most pixels reach the reference's plane exactly."""
+    a half-sweep reads only the other colour, so it is deterministic; from the
+    reference's initial state most pixels reach exactly the reference's plane."""
     z = init_probe
     images, depths, cams, params, st = golden.init_state(z, mode)
-    ora.random_init(images, cams, params, st, golden.INIT_RUN_SEED, 0)
+    ora.random_init(images, cams, params, st, golden.INIT_RUN_SEED, 0)  # the draw counters
+    st.planes[:] = z[f"ref_{name}_planes"]
+    st.costs[:] = z[f"ref_{name}_costs"]
+    st.selected_views[:] = z[f"ref_{name}_selected"]
+    if f"ref_{name}_confidences" in z:
+        st.confidences[:] = z[f"ref_{name}_confidences"]
     for h in range(n_half):
         ora.half_sweep(images, depths, cams, params, st, h % 2, h // 2, golden.INIT_RUN_SEED, 0)
     rp = z[f"ref_{name}_h{n_half}_planes"]
@@ -383,4 +389,4 @@ def test_half_sweeps_match_reference(init_probe, name, mode, n_half):
     same = np.abs(st.planes - rp).max(axis=2) <= 1e-5 * np.maximum(1.0, np.abs(rp).max(axis=2))
     assert same[updated & interior].mean() >= SWEEP_MIN_SAME[(name, n_half)], same[updated & interior].mean()
     if n_half == 1:  # pixels of the other colour keep the initial planes
-        assert same[~updated].mean() >= 0.999
+        assert same[~updated].all()
