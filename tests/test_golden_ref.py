@@ -360,10 +360,14 @@ def test_random_init_matches_reference(init_probe, name, mode):
 # 6-pixel border band.  The rest of the interior are candidates whose costs tie
 # within rounding.  Inside the band the reference reads an unassigned
 # plane_hypotheses_now (HPM.cu:1844) whenever its minimum-cost direction lies
-# outside the image; what the compiled code holds there is not a value of the
-# algorithm, so those pixels are measured, not required.
+# outside the image and writes what the register held: normals such as
+# (8.1e8, 4.6e-41, 2.8e-45).  Those pixels are counted; on the band's pixels
+# where the reference wrote a unit normal, the agreement is required to the
+# second bound.
 SWEEP_MIN_SAME = {("photometric", 1): 0.97, ("photometric", 2): 0.92, ("geometric", 1): 0.97,
                   ("mandatory", 1): 0.97, ("prior", 1): 0.99}
+SWEEP_MIN_SAME_BAND = {("photometric", 1): 0.8, ("photometric", 2): 0.6, ("geometric", 1): 0.75,
+                       ("mandatory", 1): 0.88, ("prior", 1): 0.98}
 
 
 @pytest.mark.parametrize("name,mode,n_half", golden.SWEEP_CASES, ids=[f"{c[0]}-h{c[2]}" for c in golden.SWEEP_CASES])
@@ -388,5 +392,12 @@ def test_half_sweeps_match_reference(init_probe, name, mode, n_half):
     interior = (xs >= 6) & (xs < W - 6) & (ys >= 6) & (ys < H - 6)
     same = np.abs(st.planes - rp).max(axis=2) <= 1e-5 * np.maximum(1.0, np.abs(rp).max(axis=2))
     assert same[updated & interior].mean() >= SWEEP_MIN_SAME[(name, n_half)], same[updated & interior].mean()
+    norm = np.linalg.norm(rp[..., :3].astype(np.float64), axis=2)
+    unit = np.isfinite(norm) & (np.abs(norm - 1.0) <= 1e-3)
+    band = updated & ~interior & unit
+    assert same[band].mean() >= SWEEP_MIN_SAME_BAND[(name, n_half)], same[band].mean()
+    # the oracle's own planes stay unit planes everywhere
+    on = np.linalg.norm(st.planes[..., :3].astype(np.float64), axis=2)
+    assert (np.abs(on - 1.0) <= 1e-3).all()
     if n_half == 1:  # pixels of the other colour keep the initial planes
         assert same[~updated].all()
