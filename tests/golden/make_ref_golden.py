@@ -18,7 +18,8 @@ The functions probed (HPM.cu line ranges):
   ComputeTexture                                  349-373
   JBU_cu, JBU_cu_prior (raw kernel output)        3037-3197 upsampling 64x48 -> 128x96
   RandomInitialization, five modes                567-763   a 64x48 view, 4 sources
-  + the first one or two half-sweeps              2793-2827 photometric, geometric, mandatory, prior
+  + the first one or two half-sweeps              2793-2827 photometric, geometric, mandatory, prior,
+                                                            hierarchy
 
 The scene is 5 views of 128x96 (seed 11, 4 sources).  Its grey images are
 integers (stored as uint8) and its depth maps are the ground truth rounded to
@@ -80,7 +81,7 @@ def make_jbu_inputs() -> dict:
 INIT_W, INIT_H, INIT_SEED, INIT_RUN_SEED = 64, 48, 12, 7
 INIT_CASES = (("photometric", 0), ("geometric", 1), ("mandatory", 1 | 4 | 32), ("prior", 2), ("hierarchy", 8 | 16))
 SWEEP_CASES = (("photometric", 0, 1), ("photometric", 0, 2), ("geometric", 1, 1), ("mandatory", 1 | 4 | 32, 1),
-               ("prior", 2, 1))  # (name, mode, half-sweeps)
+               ("prior", 2, 1), ("hierarchy", 8 | 16, 1))  # (name, mode, half-sweeps)
 
 
 def make_init_inputs() -> dict:
