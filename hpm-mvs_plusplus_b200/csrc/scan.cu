@@ -21,7 +21,9 @@
 //   3. marks become permanent, confidences take the value of the last pixel
 //      that marked them (atomicMax), points are compacted in raster order.
 // Arithmetic mirrors the host code of the reference (g++ without -ffast-math):
-// float geometry, double where exp/fabs/pow promote.  No implicit contraction.
+// float geometry, double where pow(float, int) promotes; exp(float) is the
+// float function there (the double exp rounded to float here).  No implicit
+// contraction.
 #include "aux_kernels.cuh"
 #include "ctx.hpp"
 
@@ -110,7 +112,8 @@ __global__ void k_candidates(const ScanView* __restrict__ views, int i, const in
                     if (reproj < 2.0f && rel < 0.01f && ang < 0.174533f) {
                         const float idx = reproj + 200 * rel + ang * 10;
                         T |= 1u << j;
-                        wexp[(size_t)q * n_ngb + j] = exp((double)(-idx));
+                        // exp(float) of the reference's host code: the float function
+                        wexp[(size_t)q * n_ngb + j] = (double)(float)exp((double)(-idx));
                     }
                 }
             }

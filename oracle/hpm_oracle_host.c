@@ -8,9 +8,12 @@
  * (main.cpp:452-454).
  *
  * These loops run on the host in the reference (compiled by g++ without
- * -ffast-math).  In those translation units `exp(float)`, `fabs(float)` and
- * `pow(float, int)` resolve to the double versions, so the restatement
- * promotes to double exactly where the reference does.
+ * -ffast-math).  In those translation units the CUDA headers bring <math.h>'s
+ * overloads into the global namespace, so `exp(float)`, `fabs(float)` and
+ * `sqrt(float)` are the float functions while `pow(float, int)` promotes to
+ * double (checked by compiling main.cpp's includes, oracle/ref_host.mk).  The
+ * restatement rounds where the reference rounds: the float exp is the double
+ * exp rounded to float.
  */
 #include "hpm_oracle.h"
 
@@ -124,7 +127,7 @@ static int64_t consistency_scan(int kind, int num_views, const hpm_camera *cams,
                         if (reproj < 2.0f && rel < 0.01f && ang < 0.174533f) {
                             used_x[j] = sc; used_y[j] = sr;
                             const float idx = reproj + 200 * rel + ang * 10;
-                            dyn = (float)((double)dyn + exp((double)(-idx)));
+                            dyn = dyn + (float)exp((double)(-idx)); /* float exp, float sum */
                             n_cons++;
                         }
                     }

@@ -1,0 +1,3 @@
+// CHECKER ONLY: see ../../cv_host.hpp
+#pragma once
+#include "../../cv_host.hpp"
