@@ -28,7 +28,7 @@ $(OUT)/host_HPM.o: $(REF)/HPM.cpp $(REF)/main.h $(REF)/HPM.h $(SHIM)
 	@mkdir -p $(OUT)
 	$(HOSTCC) $(FLAGS) -c $< -o $@
 
-$(OUT)/host_driver.o: ref_host_driver.cpp $(REF)/main.h $(SHIM)
+$(OUT)/host_driver.o: ref_host_driver.cpp $(REF)/main.h $(REF)/HPM.h $(SHIM)
 	@mkdir -p $(OUT)
 	$(HOSTCC) $(FLAGS) -c $< -o $@
 

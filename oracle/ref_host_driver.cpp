@@ -1,6 +1,8 @@
 // CHECKER ONLY: runs two host stages of the reference's own main.cpp,
 // ConfidenceEvaluation (main.cpp:959-1109) and RunFusion / RunFusion_Sky_Strict
-// (main.cpp:659-957), compiled from their sources by oracle/ref_host.mk against
+// (main.cpp:659-957), and one member of HPM.cpp, the prior's support-point
+// selection HPM::GetSupportPoints_Classify_Check (HPM.cpp:1026-1073), compiled
+// from their sources by oracle/ref_host.mk against
 // the OpenCV stand-ins of oracle/ref_shim_host.  They read a dense folder the
 // caller writes: cams/%08d_cam.txt, images/%08d.jpg.raw (see cv::imread below)
 // and HPM_MVS_plusplus/2333_%08d/{depths,depths_geom,normals}.dmb, and write
@@ -12,7 +14,10 @@
 #include <string>
 #include <vector>
 
-#include "main.h"
+#include "main.h"  // the standard headers first, so that only HPM's members open up below
+#define private public
+#include "HPM.h"
+#undef private
 
 void ConfidenceEvaluation(std::string& dense_folder, const std::vector<Problem>& problems, bool geom_consistency);
 void RunFusion(std::string& dense_folder, const std::vector<Problem>& problems, bool geom_consistency);
@@ -86,6 +91,32 @@ extern "C" __attribute__((visibility("default"))) int ref_host_fusion(const char
         return 0;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "ref_host_fusion: %s\n", e.what());
+        return -1;
+    }
+}
+
+// HPM::GetSupportPoints_Classify_Check on maps of (width*factor) x
+// (height*factor) pixels of a reference camera of width x height.  The HPM
+// object is never destroyed: its destructor releases CUDA resources.
+extern "C" __attribute__((visibility("default"))) int ref_host_support_points(
+    const Camera* cam, const float* costs, const float* confidences, const float* texture, int map_w, int map_h,
+    float factor, int* out_xy, int max_points) {
+    try {
+        static HPM* hpm = new HPM();
+        hpm->cameras.assign(1, *cam);
+        cv::Mat_<float> c(cv::Mat(map_h, map_w, CV_32FC1, const_cast<float*>(costs)));
+        cv::Mat_<float> q(cv::Mat(map_h, map_w, CV_32FC1, const_cast<float*>(confidences)));
+        cv::Mat_<float> t(cv::Mat(map_h, map_w, CV_32FC1, const_cast<float*>(texture)));
+        std::vector<cv::Point> pts;
+        hpm->GetSupportPoints_Classify_Check(pts, c, q, t, factor);
+        const int n = (int)pts.size();
+        for (int i = 0; i < n && i < max_points; ++i) {
+            out_xy[2 * i] = pts[i].x;
+            out_xy[2 * i + 1] = pts[i].y;
+        }
+        return n;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "ref_host_support_points: %s\n", e.what());
         return -1;
     }
 }

@@ -169,3 +169,31 @@ def test_fusion_matches_reference_host_code(folder, sky):
     assert np.array_equal(fused["xyz"].view(np.uint32), pts[keep, 0:3].view(np.uint32))
     assert np.array_equal(fused["n"], (n[keep] / length[keep, None]).astype(np.float32))
     assert np.array_equal(fused["rgb"], np.clip(pts[keep, 6:9], 0, 255).astype(np.uint8)[:, ::-1])
+
+
+@pytest.mark.parametrize("factor", [1.0, 0.5, 0.25])
+def test_support_points_match_reference_host_code(factor):
+    """HPM::GetSupportPoints_Classify_Check (HPM.cpp:1026-1073) on seeded cost
+    and confidence maps: the same points in the same order."""
+    import hpm_b200
+
+    W, H = 203, 157
+    w, h = int(W * np.float32(factor)), int(H * np.float32(factor))
+    rng = np.random.default_rng(int(factor * 100))
+    costs = rng.uniform(0.0, 0.4, (h, w)).astype(np.float32)
+    costs[rng.uniform(size=(h, w)) < 0.2] = 2.0
+    costs[rng.uniform(size=(h, w)) < 0.1] = np.float32(0.05)  # ties: the first pixel in scan order wins
+    conf = np.where(rng.uniform(size=(h, w)) < 0.5, 0.0, rng.uniform(0.0, 0.3, (h, w))).astype(np.float32)
+    texture = rng.uniform(0.4, 1.0, (h, w)).astype(np.float32)
+    cam = hpm_b200.Camera.make(np.diag([300.0, 300.0, 1.0]), np.eye(3), np.zeros(3), W, H, 1.0, 5.0)
+    lib = ctypes.CDLL(LIB)
+    vp = ctypes.c_void_p
+    lib.ref_host_support_points.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, vp,
+                                            ctypes.c_int]
+    cap = 2 * ((w + 4) // 5) * ((h + 4) // 5) + 8
+    out = np.zeros((cap, 2), np.int32)
+    n = lib.ref_host_support_points(ctypes.addressof(cam), costs.ctypes.data, conf.ctypes.data, texture.ctypes.data,
+                                    w, h, factor, out.ctypes.data, cap)
+    assert 0 < n <= cap
+    got = ora.support_points(costs, conf, w, h)
+    assert np.array_equal(got, out[:n])
