@@ -260,7 +260,8 @@ def main() -> None:
     for name, mode, n_half in SWEEP_CASES:
         images, depths, cams, params, st = init_state(zi, mode)
         ref_cuda.random_init(images, depths, cams, params, st, INIT_RUN_SEED, 0, n_half=n_half)
-        outs.update({f"ref_{name}_h{n_half}_planes": st.planes, f"ref_{name}_h{n_half}_costs": st.costs})
+        outs.update({f"ref_{name}_h{n_half}_planes": st.planes, f"ref_{name}_h{n_half}_costs": st.costs,
+                     f"ref_{name}_h{n_half}_selected": st.selected_views})
     np.savez_compressed(args.init_out, **zi, **outs)
     print(f"wrote {args.init_out}: {len(INIT_CASES)} modes at {INIT_W}x{INIT_H}")
 

@@ -363,10 +363,11 @@ def test_random_init_matches_reference(init_probe, name, mode):
 # outside the image and writes what the register held: normals such as
 # (8.1e8, 4.6e-41, 2.8e-45).  Those pixels are counted; on the band's pixels
 # where the reference wrote a unit normal, the agreement is required to the
-# second bound.
+# second bound, set below the measured rates because the register contents,
+# and so the band's planes, change from one reference run to the next.
 SWEEP_MIN_SAME = {("photometric", 1): 0.97, ("photometric", 2): 0.92, ("geometric", 1): 0.97,
                   ("mandatory", 1): 0.97, ("prior", 1): 0.99, ("hierarchy", 1): 0.96}
-SWEEP_MIN_SAME_BAND = {("photometric", 1): 0.8, ("photometric", 2): 0.6, ("geometric", 1): 0.75,
+SWEEP_MIN_SAME_BAND = {("photometric", 1): 0.65, ("photometric", 2): 0.6, ("geometric", 1): 0.75,
                        ("mandatory", 1): 0.88, ("prior", 1): 0.98, ("hierarchy", 1): 0.6}
 
 
@@ -392,6 +393,9 @@ def test_half_sweeps_match_reference(init_probe, name, mode, n_half):
     interior = (xs >= 6) & (xs < W - 6) & (ys >= 6) & (ys < H - 6)
     same = np.abs(st.planes - rp).max(axis=2) <= 1e-5 * np.maximum(1.0, np.abs(rp).max(axis=2))
     assert same[updated & interior].mean() >= SWEEP_MIN_SAME[(name, n_half)], same[updated & interior].mean()
+    if n_half == 1 and f"ref_{name}_h1_selected" in z:  # where the planes agree, so do the view masks
+        sel = st.selected_views == z[f"ref_{name}_h1_selected"]
+        assert sel[updated & interior & same].mean() >= 0.995
     norm = np.linalg.norm(rp[..., :3].astype(np.float64), axis=2)
     unit = np.isfinite(norm) & (np.abs(norm - 1.0) <= 1e-3)
     band = updated & ~interior & unit
