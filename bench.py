@@ -184,6 +184,24 @@ def view_pixel_runs(w: int, h: int, scale: int, geom_iterations: int = 3) -> int
 
 # ------------------------------------------------------------------ our arm
 
+def depth_accuracy(depths, scene, rel: float = 0.01):
+    """Share of the rendered ground truth's valid pixels whose reconstructed depth lies within `rel`
+    of it, over all views (None when the maps are not at the ground truth's size).  Computed after
+    the timed steps from the maps the last step downloaded."""
+    try:
+        ok = hit = 0
+        for d, v in zip(depths, scene.views):
+            gt = np.asarray(v.depth, np.float32)
+            if gt.shape != d.shape:
+                return None
+            m = gt > 0
+            ok += int(m.sum())
+            hit += int((np.abs(d[m] - gt[m]) <= rel * gt[m]).sum())
+        return hit / ok if ok else None
+    except Exception:
+        return None
+
+
 def run_ours(args, scene, rank, world, local_rank):
     import torch
     hb = _import_pkg()
@@ -270,6 +288,7 @@ def run_ours(args, scene, rank, world, local_rank):
     total_views = n_views * args.steps * world
     value = total_views / (dev_ms / 1e3)
     e2e = total_views / (e2e_ms / 1e3)
+    accuracy = depth_accuracy(depth_out, scene)
 
     # roofline of the dominant kernel: the checkerboard half-sweep
     fp32_peak = hb.measure_fp32_peak(local_rank)
@@ -307,13 +326,16 @@ def run_ours(args, scene, rank, world, local_rank):
         "gpu_launches": int(launches),
         "clocks": clocks,
         "roofline": roofline,
+        "accuracy": {"measure": "share of ground-truth pixels with depth within 1 %, all views, last step",
+                     "plain": accuracy},
     }
     if args.chosen_form:
-        result["chosen_form"] = chosen_form(args, ctx, step, n_views, world, device)
+        result["chosen_form"] = chosen_form(args, ctx, step, n_views, world, device, depth_out, scene)
+        result["accuracy"]["chosen_form"] = result["chosen_form"].get("accuracy")
     return result, ctx, images
 
 
-def chosen_form(args, ctx, step, n_views, world, device):
+def chosen_form(args, ctx, step, n_views, world, device, depth_out=None, scene=None):
     """The same steps with 8-bit source textures (hpm_set_texture_format(HPM_TEX_U8)), the precision
     form: the grey levels are stored exactly in a quarter of the bytes, the texture unit returns the
     filtered sample as grey / 255, and the scale-free NCC only rescales its flat-source test."""
@@ -327,6 +349,7 @@ def chosen_form(args, ctx, step, n_views, world, device):
     torch.cuda.synchronize()
     evs = [step()[0] for _ in range(args.steps)]
     torch.cuda.synchronize()
+    accuracy = depth_accuracy(depth_out, scene) if depth_out is not None and scene is not None else None
     ctx.set_texture_format(hb.TEX_F32)
     dev_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
     e2e_ms = sum(e[0].elapsed_time(e[3]) for e in evs)
@@ -335,7 +358,7 @@ def chosen_form(args, ctx, step, n_views, world, device):
     return {"form": "8-bit source textures (cost error against the FP64 exact-bilinear cost as for float "
                     "textures; same accuracy against the rendered ground truth, tests/test_gpu_texf16.py)",
             "value": total_views / (float(t[0]) / 1e3), "e2e": total_views / (float(t[1]) / 1e3),
-            "unit": UNIT, "ms_per_step": float(t[0]) / args.steps}
+            "unit": UNIT, "ms_per_step": float(t[0]) / args.steps, "accuracy": accuracy}
 
 
 def max_over_ranks(values, world: int, device):
