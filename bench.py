@@ -471,12 +471,17 @@ def time_reference_host_stages(L, srcs, folder):
             fh.write(img.tobytes())
         res = os.path.join(folder, "HPM_MVS_plusplus", f"2333_{i:08d}")
         os.makedirs(res, exist_ok=True)
-        for name, a in (("depths.dmb", L["depth"][i]), ("depths_geom.dmb", L["depth"][i]),
-                        ("normals.dmb", L["normal"][i])):
+        for name, a in (("depths.dmb", L["depth"][i]), ("normals.dmb", L["normal"][i])):
             a = np.ascontiguousarray(a, np.float32)
             with open(os.path.join(res, name), "wb") as fh:
                 fh.write(np.array([1, a.shape[0], a.shape[1], 1 if a.ndim == 2 else a.shape[2]], np.int32).tobytes())
                 fh.write(a.tobytes())
+        # the geometric maps are the same maps here: a second name for the same file
+        try:
+            os.link(os.path.join(res, "depths.dmb"), os.path.join(res, "depths_geom.dmb"))
+        except OSError:
+            import shutil
+            shutil.copyfile(os.path.join(res, "depths.dmb"), os.path.join(res, "depths_geom.dmb"))
     off = np.zeros(n + 1, np.int32)
     for i, sl in enumerate(srcs):
         off[i + 1] = off[i] + len(sl)
