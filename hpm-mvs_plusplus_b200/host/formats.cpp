@@ -1,4 +1,5 @@
 #include "formats.hpp"
+#include "hpm_host.h"
 
 #include <algorithm>
 #include <cfloat>
@@ -134,3 +135,10 @@ bool write_fused_ply(const std::string& path, const hpm_point* pts, size_t n, si
 }
 
 }  // namespace hpm_host
+
+extern "C" int hpm_write_ply(const char* path, const hpm_point* pts, size_t n, int fused, size_t* written) {
+    if (!path || (!pts && n)) return -1;
+    if (fused) return hpm_host::write_fused_ply(path, pts, n, written) ? 0 : -1;
+    if (written) *written = n;
+    return hpm_host::write_points_ply(path, pts, n) ? 0 : -1;
+}

@@ -8,7 +8,8 @@ perturbed depths and holes), runs the reference stage on it, and compares
 what it wrote -- confidence.dmb, fused.ply, HPM_MVS_plusplus(_mask).ply --
 with the oracle's restatement (ora_confidence_eval, ora_fusion) on the same
 maps.  Both are IEEE host code.  Point sets, order, coordinates, normals and
-colours are compared bit for bit.  A confidence value sums float exp terms:
+colours are compared bit for bit, and the library's own PLY writer
+(hpm_write_ply) reproduces the reference's files byte for byte.  A confidence value sums float exp terms:
 the reference's exp(float) is glibc's expf, accurate to 0.502 ulp, which in
 about 0.07 % of evaluations rounds the other way from the correctly rounded
 value the oracle and the CUDA path use.  Confidences are therefore required on
@@ -27,6 +28,7 @@ from conftest import scene_cams
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libhpmref_host.so")
+HOST_LIB = os.path.join(os.path.dirname(HERE), "hpm-mvs_plusplus_b200", "_build", "libhpm_host.so")
 if not os.path.exists(LIB):
     pytest.skip("reference host build oracle/_ref/libhpmref_host.so not present", allow_module_level=True)
 
@@ -169,6 +171,16 @@ def test_fusion_matches_reference_host_code(folder, sky):
     assert np.array_equal(fused["xyz"].view(np.uint32), pts[keep, 0:3].view(np.uint32))
     assert np.array_equal(fused["n"], (n[keep] / length[keep, None]).astype(np.float32))
     assert np.array_equal(fused["rgb"], np.clip(pts[keep, 6:9], 0, 255).astype(np.uint8)[:, ::-1])
+    # the library's writers (hpm_write_ply, include/hpm_host.h) give the same files byte for byte
+    host = ctypes.CDLL(HOST_LIB)
+    host.hpm_write_ply.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_size_t)]
+    pts = np.ascontiguousarray(pts, np.float32)
+    for fused_flag, name in ((0, "HPM_MVS_plusplus_mask.ply" if sky else "HPM_MVS_plusplus.ply"), (1, "fused.ply")):
+        mine = f["root"] / f"ours_{sky}_{name}"
+        n = ctypes.c_size_t()
+        assert host.hpm_write_ply(str(mine).encode(), pts.ctypes.data, len(pts), fused_flag, ctypes.byref(n)) == 0
+        assert (out / name).read_bytes() == mine.read_bytes(), name
 
 
 @pytest.mark.parametrize("factor", [1.0, 0.5, 0.25])
