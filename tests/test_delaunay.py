@@ -66,3 +66,40 @@ def test_support_point_grid_agreement():
     inter = len(ours & ref)
     print(f"support-point grid: ours {len(ours)}, cv2 {len(ref)}, shared {inter / max(1, len(ref)):.3f}")
     assert inter >= 0.9 * len(ref)
+
+
+def test_plane_fits_match_opencv_svd():
+    """HPM::GetPriorPlaneParams (HPM.cpp:1132-1166) fits each triangle's plane with
+    cv::SVD::solveZ on the 3x4 float matrix of its camera-frame points.  The
+    restatement takes the exact null space in double; against OpenCV's own float
+    SVD (cv2.SVDecomp, full UV, last row of V^T, then the reference's sign rule and
+    normalisation) the plane parameters agree to 1e-4 relative."""
+    import hpm_oracle as ora
+    from hpm_b200 import synth
+    from conftest import scene_cams
+
+    sc = synth.make_scene(n_views=5, width=320, height=240, seed=1, n_src=4)
+    cam = scene_cams(sc)[0]
+    depth = np.where(sc.views[0].depth > 0, sc.views[0].depth, 6.0).astype(np.float32)
+    rng = np.random.default_rng(0)
+    pts = np.unique(np.stack([rng.integers(0, 320, 900), rng.integers(0, 240, 900)], 1), axis=0).astype(np.int32)
+    tris = np.asarray(hpm_b200.delaunay(pts, 320, 240), np.int32).reshape(-1, 6)
+    _, planes, _, _ = ora.planar_prior(tris, depth, cam, 1.0, 0.1, 100.0, 0)
+    K = np.array(cam.K, np.float32).reshape(3, 3)
+    f32 = np.float32
+
+    def point(x, y):  # Get3DPointonRefCam (HPM.cpp:258-267), float arithmetic
+        d = depth[y, x]
+        return [f32(d * f32(f32(x) - K[0, 2])) / K[0, 0], f32(d * f32(f32(y) - K[1, 2])) / K[1, 1], d]
+
+    worst = 0.0
+    for t, pl in zip(tris, planes):
+        A = np.ones((3, 4), np.float32)
+        for r in range(3):
+            A[r, :3] = point(t[2 * r], t[2 * r + 1])
+        B = cv2.SVDecomp(A, flags=cv2.SVD_FULL_UV)[2][-1].astype(np.float32)
+        norm = f32(np.sqrt(np.float64(B[0]) ** 2 + np.float64(B[1]) ** 2 + np.float64(B[2]) ** 2))
+        ref = (B / (-norm if B[3] < 0 else norm)).astype(np.float32)
+        worst = max(worst, float(np.abs(ref - pl).max()) / max(1.0, abs(float(ref[3]))))
+    print(f"plane fits vs cv2 SVD over {len(tris)} triangles: worst relative difference {worst:.2e}")
+    assert worst <= 1e-4
