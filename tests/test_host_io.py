@@ -144,3 +144,45 @@ def test_scene_folder_formats(tmp_path):
     # images are PNG bytes under .jpg names, which imread sniffs
     with open(tmp_path / "images" / "00000000.jpg", "rb") as fh:
         assert fh.read(8) == b"\x89PNG\r\n\x1a\n"
+
+
+def _parse_ply(raw: bytes):
+    end = raw.index(b"end_header\n") + len(b"end_header\n")
+    header = raw[:end].decode()
+    n = int(header.split("element vertex ")[1].split()[0])
+    fused = "property float nx" in header
+    dt = np.dtype([("xyz", "<f4", 3), ("n", "<f4", 3), ("rgb", "u1", 3)]) if fused else \
+        np.dtype([("xyz", "<f4", 3), ("rgb", "u1", 3)])
+    assert len(raw) == end + n * dt.itemsize
+    return np.frombuffer(raw[end:], dt)
+
+
+def test_write_ply_contracts(host, tmp_path):
+    """hpm_write_ply (ExportPointCloud / ExportFusedPointCloud, HPM.cpp:410-498):
+    non-finite coordinates become 0 in the plain file; the fused file drops points
+    with non-finite coordinates or a zero normal, makes normals unit and clamps
+    colours; misuse returns -1."""
+    host.hpm_write_ply.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_size_t)]
+    pts = np.array([
+        [1, 2, 3, 0, 0, 2, 10, 20, 30],              # ordinary point, normal of length 2
+        [np.inf, 2, 3, 0, 1, 0, 10, 20, 30],         # non-finite coordinate
+        [4, 5, 6, 0, 0, 0, 300, -5, 12.7],           # zero normal, colours out of range
+        [7, 8, 9, 3, 4, 0, 255, 128, 0],
+    ], np.float32)
+    n = ctypes.c_size_t()
+    plain = tmp_path / "plain.ply"
+    assert host.hpm_write_ply(str(plain).encode(), pts.ctypes.data, len(pts), 0, ctypes.byref(n)) == 0
+    p = _parse_ply(plain.read_bytes())
+    assert n.value == 4 and len(p) == 4
+    assert np.array_equal(p["xyz"][1], [0, 0, 0])
+    assert np.array_equal(p["rgb"][0], [30, 20, 10])  # BGR floats stored as R, G, B
+    fused = tmp_path / "fused.ply"
+    assert host.hpm_write_ply(str(fused).encode(), pts.ctypes.data, len(pts), 1, ctypes.byref(n)) == 0
+    f = _parse_ply(fused.read_bytes())
+    assert n.value == 2 and len(f) == 2
+    assert np.allclose(f["n"], [[0, 0, 1], [0.6, 0.8, 0]])
+    assert np.array_equal(f["rgb"][1], [0, 128, 255])
+    assert host.hpm_write_ply(None, pts.ctypes.data, len(pts), 0, None) == -1
+    assert host.hpm_write_ply(str(tmp_path / "x.ply").encode(), None, 3, 0, None) == -1
+    assert host.hpm_write_ply(str(tmp_path / "no_such_dir" / "x.ply").encode(), pts.ctypes.data, 1, 1, None) == -1
