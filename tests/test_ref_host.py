@@ -80,9 +80,15 @@ def _read_ply(path):
     return np.frombuffer(raw[end:end + n * dt.itemsize], dt)
 
 
-@pytest.fixture(scope="module")
-def folder(tmp_path_factory, small_scene):
-    return write_folder(tmp_path_factory.mktemp("dense"), small_scene)
+@pytest.fixture(scope="module", params=["even", "uneven"])
+def folder(request, tmp_path_factory, small_scene):
+    """The 5-view 160x120 scene, and a 5-view scene whose views differ in size."""
+    if request.param == "even":
+        return write_folder(tmp_path_factory.mktemp("dense"), small_scene)
+    from hpm_b200 import synth
+    scene = synth.make_scene(n_views=5, width=160, height=120, seed=2, n_src=4,
+                             sizes=[(160, 120), (144, 108), (176, 132), (160, 100), (120, 120)])
+    return write_folder(tmp_path_factory.mktemp("dense_uneven"), scene)
 
 
 def write_folder(root, small_scene):
