@@ -118,7 +118,7 @@ class Camera(ctypes.Structure):
 
 
 class Params(ctypes.Structure):
-    """hpm_params (PatchMatchParams, HPM.h:229-252)."""
+    """hpm_params (PatchMatchParams, HPM.h:32-55)."""
 
     _fields_ = [
         ("max_iterations", ctypes.c_int32),

@@ -350,6 +350,10 @@ int hpm_fuse(hpm_ctx* ctx, int n_views, const int32_t* src_off, const int32_t* s
     if (!ctx) return HPM_E_INVALID;
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     if (n_views < 1 || n_views > HPM_MAX_VIEWS) return c->fail(HPM_E_INVALID, "hpm_fuse: bad view count");
+    // checked before the maps are read to size the point buffer
+    if (depth_kind != HPM_MAP_DEPTH && depth_kind != HPM_MAP_DEPTH_GEOM)
+        return c->fail(HPM_E_INVALID, "hpm_fuse: depth_kind must be HPM_MAP_DEPTH or HPM_MAP_DEPTH_GEOM");
+    if (!src_off || !src_ids) return c->fail(HPM_E_INVALID, "hpm_fuse: null source lists");
     cudaSetDevice(c->device);
     size_t total = 0;
     for (int v = 0; v < n_views; ++v) total += (size_t)c->views[v].maps[depth_kind].w * c->views[v].maps[depth_kind].h;

@@ -14,7 +14,7 @@
 
 namespace hpm {
 
-constexpr int kPatchSamples = 36;   // 11x11 window, stride 2 (HPM.h:231-234)
+constexpr int kPatchSamples = 36;   // 11x11 window, stride 2 (HPM.h:34-36)
 constexpr int kPatchRadius = 5;
 constexpr int kPatchStep = 2;
 constexpr int kMarsagliaMaxTries = 4096;

@@ -198,12 +198,7 @@ __device__ __forceinline__ float range_gauss(float x, float sigma) {
 }
 
 template <int NS, int BLK, bool CNT>
-__global__ void __launch_bounds__(BLK) k_random_init(const __grid_constant__ RunArgs a) {
-    extern __shared__ float smem[];
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    Scratch<NS, BLK, CNT> s{ smem + tid };
-    const int px = blockIdx.x * blockDim.x + threadIdx.x;
-    const int py = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void init_pixel(const RunArgs& a, const Scratch<NS, BLK, CNT>& s, int px, int py) {
     const int W = a.W, H = a.H;
     if (px >= W || py >= H) return;
     const int center = py * W + px;
@@ -308,6 +303,53 @@ __global__ void __launch_bounds__(BLK) k_random_init(const __grid_constant__ Run
         a.sel[center] = sel;
     }
     a.rng[center] = rng.draw;
+}
+
+template <int NS, int BLK, bool CNT>
+__global__ void __launch_bounds__(BLK) k_random_init(const __grid_constant__ RunArgs a) {
+    extern __shared__ float smem[];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const Scratch<NS, BLK, CNT> s{ smem + tid };
+    init_pixel<NS, BLK, CNT>(a, s, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+}
+
+// ---------------------------------------------------------------- batched launches
+//
+// The batching form: the runs of several reference views (one pass of the
+// schedule over the views of a pyramid level, main.cpp:1253-1255) share one
+// launch per stage.  Their RunArgs sit in device memory; block b of the launch
+// is tile b - tile_start[k] of run k, the last run with tile_start[k] <= b.
+// A tile is the block footprint of the single-view launch, so every pixel sees
+// exactly the arithmetic of the per-view kernels.  With gridDim.x smaller than
+// the tile count the launch is persistent: each block walks the tiles b,
+// b + gridDim.x, ...  The per-view kernels launch one view at a time and wait
+// for each launch (HPM.cu:2987-3035); here the tail of one view's grid overlaps
+// the next view's tiles.
+
+__device__ __forceinline__ int batch_run_of(const int* __restrict__ tile_start, int n, int b) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(tile_start + mid) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int NS, int BLK, bool CNT>
+__global__ void __launch_bounds__(BLK) k_random_init_batch(const RunArgs* __restrict__ args,
+                                                           const int* __restrict__ tile_start, int n) {
+    extern __shared__ float smem[];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const Scratch<NS, BLK, CNT> s{ smem + tid };
+    const int total = __ldg(tile_start + n);
+    for (int b = blockIdx.x; b < total; b += gridDim.x) {
+        const int k = batch_run_of(tile_start, n, b);
+        const RunArgs& a = args[k];
+        const int t = b - __ldg(tile_start + k);
+        const int tx = (a.W + blockDim.x - 1) / blockDim.x;
+        init_pixel<NS, BLK, CNT>(a, s, (t % tx) * blockDim.x + threadIdx.x, (t / tx) * blockDim.y + threadIdx.y);
+    }
 }
 
 // ---------------------------------------------------------------- propagation
@@ -569,12 +611,8 @@ __device__ __forceinline__ float prior_score(float final_cost, float depth_now, 
 #endif
 
 template <int NS, int BLK, bool MAND, bool CNT>
-__global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const __grid_constant__ RunArgs a, int color, int iter) {
-    extern __shared__ float smem[];
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    const Scratch<NS, BLK, CNT> s{ smem + tid };
-    const int px = blockIdx.x * blockDim.x + threadIdx.x;
-    const int pair = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void sweep_pixel(const RunArgs& a, const Scratch<NS, BLK, CNT>& s, int px, int pair,
+                                            int color, int iter) {
     const int py = 2 * pair + ((px & 1) ^ color);
     const int W = a.W, H = a.H, S = a.S;
     if (px >= W || py >= H || pair >= a.cover_pairs) return;
@@ -854,6 +892,33 @@ __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const 
     a.rng[center] = rng.draw;
 }
 
+template <int NS, int BLK, bool MAND, bool CNT>
+__global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const __grid_constant__ RunArgs a, int color, int iter) {
+    extern __shared__ float smem[];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const Scratch<NS, BLK, CNT> s{ smem + tid };
+    sweep_pixel<NS, BLK, MAND, CNT>(a, s, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y * blockDim.y + threadIdx.y,
+                                    color, iter);
+}
+
+template <int NS, int BLK, bool MAND, bool CNT>
+__global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS)
+    k_half_sweep_batch(const RunArgs* __restrict__ args, const int* __restrict__ tile_start, int n, int color,
+                       int iter) {
+    extern __shared__ float smem[];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const Scratch<NS, BLK, CNT> s{ smem + tid };
+    const int total = __ldg(tile_start + n);
+    for (int b = blockIdx.x; b < total; b += gridDim.x) {
+        const int k = batch_run_of(tile_start, n, b);
+        const RunArgs& a = args[k];
+        const int t = b - __ldg(tile_start + k);
+        const int tx = (a.W + blockDim.x - 1) / blockDim.x;
+        sweep_pixel<NS, BLK, MAND, CNT>(a, s, (t % tx) * blockDim.x + threadIdx.x,
+                                        (t / tx) * blockDim.y + threadIdx.y, color, iter);
+    }
+}
+
 __global__ void k_export(const __grid_constant__ RunArgs a) {
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int py = blockIdx.y * blockDim.y + threadIdx.y;
@@ -909,6 +974,41 @@ static cudaError_t sweep_impl(const RunArgs& a, int color, int iter, cudaStream_
     return cudaGetLastError();
 }
 
+template <int NS, bool CNT>
+static cudaError_t init_batch_impl(const BatchLaunch& bl, cudaStream_t st) {
+    constexpr int BLK = 128;
+    const size_t shm = sizeof(float) * Scratch<NS, BLK>::kWords * BLK;
+    auto k = k_random_init_batch<NS, BLK, CNT>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    if (e != cudaSuccess) return e;
+    const int grid = bl.grid_blocks > 0 && bl.grid_blocks < bl.tiles ? bl.grid_blocks : bl.tiles;
+    k<<<grid, dim3(16, 8), shm, st>>>(bl.args, bl.tile_start, bl.n);
+    return cudaGetLastError();
+}
+
+template <int NS, bool MAND, bool CNT>
+static cudaError_t sweep_batch_impl(const BatchLaunch& bl, int color, int iter, cudaStream_t st) {
+    constexpr int BLK = block_threads<NS>();
+    const size_t shm = sizeof(float) * Scratch<NS, BLK>::kWords * BLK;
+    auto k = k_half_sweep_batch<NS, BLK, MAND, CNT>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    if (e != cudaSuccess) return e;
+    const int grid = bl.grid_blocks > 0 && bl.grid_blocks < bl.tiles ? bl.grid_blocks : bl.tiles;
+    k<<<grid, dim3(32, BLK / 32), shm, st>>>(bl.args, bl.tile_start, bl.n, color, iter);
+    return cudaGetLastError();
+}
+
+template <int NS, bool MAND, bool CNT>
+static int sweep_batch_occupancy() {
+    constexpr int BLK = block_threads<NS>();
+    const size_t shm = sizeof(float) * Scratch<NS, BLK>::kWords * BLK;
+    auto k = k_half_sweep_batch<NS, BLK, MAND, CNT>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm) != cudaSuccess) return 0;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, BLK, shm) != cudaSuccess) return 0;
+    return blocks;
+}
+
 template <bool CNT>
 static cudaError_t init_dispatch(const RunArgs& a, cudaStream_t st) {
     if (a.S <= 4) return init_impl<4, CNT>(a, st);
@@ -935,6 +1035,43 @@ cudaError_t launch_half_sweep(const RunArgs& a, int color, int iter, cudaStream_
         return mand ? sweep_dispatch<true, true>(a, color, iter, st) : sweep_dispatch<false, true>(a, color, iter, st);
     return mand ? sweep_dispatch<true, false>(a, color, iter, st) : sweep_dispatch<false, false>(a, color, iter, st);
 }
+
+template <bool CNT>
+static cudaError_t init_batch_dispatch(const BatchLaunch& bl, cudaStream_t st) {
+    if (bl.max_s <= 4) return init_batch_impl<4, CNT>(bl, st);
+    if (bl.max_s <= 10) return init_batch_impl<10, CNT>(bl, st);
+    if (bl.max_s <= 16) return init_batch_impl<16, CNT>(bl, st);
+    return init_batch_impl<31, CNT>(bl, st);
+}
+
+cudaError_t launch_random_init_batch(const BatchLaunch& bl, cudaStream_t st) {
+    return bl.count ? init_batch_dispatch<true>(bl, st) : init_batch_dispatch<false>(bl, st);
+}
+
+template <bool MAND, bool CNT>
+static cudaError_t sweep_batch_dispatch(const BatchLaunch& bl, int color, int iter, cudaStream_t st) {
+    if (bl.max_s <= 4) return sweep_batch_impl<4, MAND, CNT>(bl, color, iter, st);
+    if (bl.max_s <= 10) return sweep_batch_impl<10, MAND, CNT>(bl, color, iter, st);
+    if (bl.max_s <= 16) return sweep_batch_impl<16, MAND, CNT>(bl, color, iter, st);
+    return sweep_batch_impl<31, MAND, CNT>(bl, color, iter, st);
+}
+
+cudaError_t launch_half_sweep_batch(const BatchLaunch& bl, int color, int iter, cudaStream_t st) {
+    if (bl.count)
+        return bl.mand ? sweep_batch_dispatch<true, true>(bl, color, iter, st)
+                       : sweep_batch_dispatch<false, true>(bl, color, iter, st);
+    return bl.mand ? sweep_batch_dispatch<true, false>(bl, color, iter, st)
+                   : sweep_batch_dispatch<false, false>(bl, color, iter, st);
+}
+
+int half_sweep_batch_occupancy(int max_s, bool mand) {
+    if (max_s <= 4) return mand ? sweep_batch_occupancy<4, true, false>() : sweep_batch_occupancy<4, false, false>();
+    if (max_s <= 10) return mand ? sweep_batch_occupancy<10, true, false>() : sweep_batch_occupancy<10, false, false>();
+    if (max_s <= 16) return mand ? sweep_batch_occupancy<16, true, false>() : sweep_batch_occupancy<16, false, false>();
+    return mand ? sweep_batch_occupancy<31, true, false>() : sweep_batch_occupancy<31, false, false>();
+}
+
+int half_sweep_block_threads(int max_s) { return max_s <= 10 ? 128 : (max_s <= 16 ? 64 : 32); }
 
 cudaError_t launch_export(const RunArgs& a, cudaStream_t st) {
     dim3 block(32, 8), grid((a.W + 31) / 32, (a.H + 7) / 8);

@@ -59,6 +59,27 @@ cudaError_t launch_export(const RunArgs& a, cudaStream_t st);
 cudaError_t launch_eval_costs(const RunArgs& a, int n, const int32_t* px, const float4* planes, float* out,
                               cudaStream_t st);
 
+// One launch of the batching form over several runs (pm_kernels.cu): the runs'
+// RunArgs and the prefix sums of their tile counts (n + 1 entries) in device
+// memory.  Tiles are the per-view launches' blocks: 16 x 8 pixels for the
+// initialisation, 32 x (block_threads / 32) row pairs for a half-sweep.
+struct BatchLaunch {
+    const RunArgs* args;
+    const int* tile_start;
+    int n;            // runs
+    int tiles;        // tile_start[n]
+    int max_s;        // largest source count (kernel specialisation)
+    int grid_blocks;  // 0 or >= tiles: one block per tile; else a persistent grid of this many blocks
+    bool mand;        // mandatory-consistency kernel
+    bool count;       // counting build (hyp_count of every run set)
+};
+
+cudaError_t launch_random_init_batch(const BatchLaunch& bl, cudaStream_t st);
+cudaError_t launch_half_sweep_batch(const BatchLaunch& bl, int color, int iter, cudaStream_t st);
+// Resident blocks per SM of the batched half-sweep kernel, and its block size.
+int half_sweep_batch_occupancy(int max_s, bool mand);
+int half_sweep_block_threads(int max_s);
+
 // Rows covered by the checkerboard launch of RunPatchMatch (HPM.cu:3004-3011):
 // the grid spans ceil(floor(H/2)/16)*16 row pairs.
 inline int covered_row_pairs(int H) { return ((H / 2 + 15) / 16) * 16; }

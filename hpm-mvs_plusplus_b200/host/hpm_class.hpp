@@ -1,4 +1,4 @@
-// The reference's host-side `HPM` class (HPM.h:254-337) rebuilt on the C ABI
+// The reference's host-side `HPM` class (HPM.h:57-140) rebuilt on the C ABI
 // of libhpm_cuda.so, with its method names and call order, for callers written
 // against it (ProcessProblem, main.cpp:237-634).  cv::Mat_ arguments become the
 // small row-major `Map` below; all views share one process-wide context, so

@@ -346,10 +346,12 @@ int Jpeg::decode(std::vector<uint8_t>& bgr, int& W, int& H) {
         const size_t seg = pos_ + 4;
         if (seg + len - 2 > n_ || len < 2) return fail("JPEG: truncated segment");
         if (marker == 0xDB) {  // DQT
+            const size_t end = seg + len - 2;
             size_t p = seg;
-            while (p < seg + len - 2) {
+            while (p < end) {
                 const int pq = d_[p] >> 4, tq = d_[p] & 15;
-                if (tq > 3) return fail("JPEG: bad quantisation table id");
+                if (tq > 3 || pq > 1) return fail("JPEG: bad quantisation table id or precision");
+                if (p + 1 + 64 * (pq + 1) > end) return fail("JPEG: truncated quantisation table");
                 ++p;
                 for (int k = 0; k < 64; ++k) {
                     q_[tq][k] = pq ? (uint16_t)read_u16(p + 2 * k) : d_[p + k];
@@ -357,21 +359,27 @@ int Jpeg::decode(std::vector<uint8_t>& bgr, int& W, int& H) {
                 p += pq ? 128 : 64;
             }
         } else if (marker == 0xC4) {  // DHT
+            const size_t end = seg + len - 2;
             size_t p = seg;
-            while (p < seg + len - 2) {
+            while (p < end) {
                 const int tc = d_[p] >> 4, th = d_[p] & 15;
                 if (th > 3 || tc > 1) return fail("JPEG: bad Huffman table id");
+                if (p + 17 > end) return fail("JPEG: truncated Huffman table");
                 int total = 0;
                 for (int i = 0; i < 16; ++i) total += d_[p + 1 + i];
+                if (p + 17 + (size_t)total > end) return fail("JPEG: truncated Huffman table");
                 if (build_huffman(tc ? ac_[th] : dc_[th], d_ + p + 1, d_ + p + 17, total)) return -1;
                 p += 17 + total;
             }
         } else if (marker == 0xC0 || marker == 0xC1) {  // SOF0 / SOF1
+            if (frame) return fail("JPEG: more than one frame header");
+            if (len - 2 < 6) return fail("JPEG: truncated frame header");
             if (d_[seg] != 8) return fail("JPEG: only 8-bit samples are supported");
             height_ = read_u16(seg + 1);
             width_ = read_u16(seg + 3);
             const int nc = d_[seg + 5];
             if (width_ <= 0 || height_ <= 0 || (nc != 1 && nc != 3)) return fail("JPEG: unsupported frame");
+            if (6 + 3 * nc > len - 2) return fail("JPEG: truncated frame header");
             comps_.resize(nc);
             for (int i = 0; i < nc; ++i) {
                 Component& c = comps_[i];
@@ -393,15 +401,21 @@ int Jpeg::decode(std::vector<uint8_t>& bgr, int& W, int& H) {
         } else if (marker >= 0xC2 && marker <= 0xCF && marker != 0xC4 && marker != 0xC8 && marker != 0xCC) {
             return fail("JPEG: progressive, lossless or arithmetic-coded files are not supported");
         } else if (marker == 0xDD) {  // DRI
+            if (len - 2 < 2) return fail("JPEG: truncated restart interval");
             restart_ = read_u16(seg);
         } else if (marker == 0xDA) {  // SOS
             if (!frame) return fail("JPEG: scan before frame header");
+            if (len - 2 < 1) return fail("JPEG: truncated scan header");
             const int ns = d_[seg];
-            std::vector<Component> scan;
+            if (1 + 2 * ns > len - 2) return fail("JPEG: truncated scan header");
             for (int i = 0; i < ns; ++i) {
                 const int cid = d_[seg + 1 + 2 * i], t = d_[seg + 2 + 2 * i];
+                const int td = t >> 4, ta = t & 15;
+                if (td > 3 || ta > 3) return fail("JPEG: bad Huffman table selector");
+                bool found = false;
                 for (auto& c : comps_)
-                    if (c.id == cid) { c.td = t >> 4; c.ta = t & 15; }
+                    if (c.id == cid) { c.td = td; c.ta = ta; found = true; }
+                if (!found) return fail("JPEG: scan names an unknown component");
             }
             if (ns != (int)comps_.size()) return fail("JPEG: non-interleaved multi-scan files are not supported");
             pos_ = seg + len - 2;

@@ -2,12 +2,12 @@
  * C ABI of libhpm_cuda.so: the drop-in boundary of the HPM-MVS++ depth/normal
  * hot path.
  *
- * The reference exposes this path as the C++ class `HPM` (HPM.h:58-170) plus
+ * The reference exposes this path as the C++ class `HPM` (HPM.h:57-140) plus
  * `RunJBU` (HPM.h:20), `ConfidenceEvaluation` and `RunFusion` (main.cpp:823-1109).
  * Each of those uploads its inputs, runs, downloads and goes through .dmb files
  * on disk.  This ABI keeps every view's images and "dmb maps" resident on the
  * GPU inside one context, so a whole reconstruction schedule runs without
- * host round trips; the host C++ `HPM` class (host/hpm.hpp) is rebuilt on top.
+ * host round trips; the host C++ `HPM` class (host/hpm_class.hpp) is rebuilt on top.
  *
  * Conventions: plain pointers and sizes, host memory unless a name says
  * `_device`; every function returns 0 on success or a positive HPM_E* code and

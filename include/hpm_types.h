@@ -5,7 +5,7 @@
  * hpm_camera  mirrors `struct Camera` of HPM-MVS++ (main.h:39-47) byte for byte:
  *             K[9], R[9], t[3] (world->camera: x_cam = R x_world + t),
  *             height, width, depth_min, depth_max  -> 100 bytes.
- * hpm_params  carries the fields of `PatchMatchParams` (HPM.h:229-252) that the
+ * hpm_params  carries the fields of `PatchMatchParams` (HPM.h:32-55) that the
  *             hot path reads, as ints/floats so the struct is ABI stable.
  */
 #ifndef HPM_TYPES_H
@@ -27,7 +27,7 @@ typedef struct hpm_camera {
     float depth_max;
 } hpm_camera;
 
-/* Mode bits of one PatchMatch run (the bools of PatchMatchParams, HPM.h:244-251). */
+/* Mode bits of one PatchMatch run (the bools of PatchMatchParams, HPM.h:49-54). */
 enum {
     HPM_MODE_GEOM      = 1u << 0, /* geom_consistency  */
     HPM_MODE_PRIOR     = 1u << 1, /* prior_consistency */

@@ -3,8 +3,11 @@
 # (CMakeLists.txt:10, arch changed from sm_86), plus ref_driver.cu, into
 # oracle/_ref/libhpmref.so.  OpenCV is replaced by type stand-ins
 # (ref_shim/opencv2) and curand seeding by ref_shim/ref_rng.h; no reference
-# source is copied.   make -f ref_build.mk
-REF ?= /root/reference
+# source is copied.   make -f ref_build.mk REF=<reference source tree>
+# REF: the reference's source tree (HPM.cu, HPM.h, main.h, main.cpp, HPM.cpp); no default
+ifndef REF
+$(error set REF to the reference's source tree: make -f ref_build.mk REF=<reference source tree>)
+endif
 NVCC ?= /usr/local/cuda/bin/nvcc
 HOSTCC := $(shell test -x /usr/bin/g++ && echo /usr/bin/g++ || echo g++)
 OUT := _ref

@@ -10,8 +10,11 @@
 # (CMakeLists.txt:11-19); -O2 changes no IEEE result on x86-64 (no FMA
 # contraction without -mfma).  OpenMP is left off so that ExportPointCloud's
 # parallel loop (HPM.cpp:464) writes the points in order.
-#   make -f ref_host.mk
-REF ?= /root/reference
+#   make -f ref_host.mk REF=<reference source tree>
+# REF: the reference's source tree (HPM.cu, HPM.h, main.h, main.cpp, HPM.cpp); no default
+ifndef REF
+$(error set REF to the reference's source tree: make -f ref_host.mk REF=<reference source tree>)
+endif
 HOSTCC := $(shell test -x /usr/bin/g++ && echo /usr/bin/g++ || echo g++)
 OUT := _ref
 FLAGS := -std=c++14 -O2 -fPIC -ffunction-sections -fdata-sections -fvisibility=hidden -w \

@@ -227,7 +227,7 @@ def main() -> None:
     import ref_cuda
 
     if not ref_cuda.available():
-        raise SystemExit("oracle/_ref/libhpmref.so is not built (make -C oracle -f ref_build.mk)")
+        raise SystemExit("oracle/_ref/libhpmref.so is not built (make -C oracle -f ref_build.mk REF=<reference source tree>)")
     inputs = make_inputs()
     tmp = args.out + ".inputs.npz"
     np.savez_compressed(tmp, **inputs)

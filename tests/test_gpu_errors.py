@@ -48,6 +48,9 @@ def test_misuse_is_reported_and_the_context_survives(small_scene):
         _raises(lambda: ctx.eval_costs(0, srcs, p, np.array([[-1, 0]]), np.zeros((1, 4))), "outside")
         # maps that do not exist
         _raises(lambda: ctx.get_map(3, hpm_b200.MAP_CONF), "no map")
+        # fusion of a map kind that is not a depth map, and of an out-of-range kind
+        _raises(lambda: ctx.fuse([srcs] * 5, depth_kind=hpm_b200.MAP_COST, capacity=16), "depth_kind")
+        _raises(lambda: ctx.fuse([srcs] * 5, depth_kind=99, capacity=16), "depth_kind")
         # a whole reconstruction with a bad scale
         for i, v in enumerate(small_scene.views):
             ctx.set_image(i, v.image)

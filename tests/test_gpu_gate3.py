@@ -1,0 +1,175 @@
+"""End-to-end accuracy gate, per run: the CUDA path against the reference's own
+CUDA build (HPM.cu compiled from its sources for sm_100a, oracle/_ref) from
+identical inputs.
+
+The schedule of main() (oracle/pipeline.py) is driven by the reference build:
+every PatchMatch run of every pass takes its inputs -- planes, costs,
+confidences, priors, the sources' depth maps -- from the reference's own
+earlier runs, with the host stages of the C restatement and OpenCV in between.
+Before each reference run the CUDA path (through the C ABI) runs on a copy of
+the same inputs with the same random stream, and the two results are compared
+pixel by pixel at the gate's tolerance: 0.5 % relative depth and 2 degrees of
+normal.  Disagreeing pixels are classified (tests/gate3.py).
+
+Scenes: the 5-view 1280x960 arc at --initial-image-scale 4 (320x240, 4
+sources, one level; every pass), and an 11-view 1600x1200 hemisphere with 10
+sources per view at --initial-image-scale 1 (levels 800x600 and 1600x1200:
+photometric, prior, hierarchy, geometric and mandatory passes).
+
+Also: the first two half-sweeps of a 1600x1200 run with 10 sources (the NS = 10
+kernel at the bench's size) bit for bit against the C oracle.
+"""
+from __future__ import annotations
+
+import os
+
+import cv2
+import numpy as np
+import pytest
+
+import hpm_b200
+import hpm_oracle as ora
+
+import gate3
+from conftest import scene_cams
+from cuda_runner import CudaRunner, copy_state
+
+pytestmark = pytest.mark.gpu
+
+ref_cuda = pytest.importorskip("ref_cuda")
+if not ref_cuda.available():
+    pytest.skip("reference build oracle/_ref/libhpmref.so not present", allow_module_level=True)
+
+MODE_NAMES = {0: "photometric", 2: "prior", 8: "hierarchy", 24: "hierarchy", 1: "geometric", 37: "mandatory"}
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = hpm_b200.Context(0)
+    yield c
+    c.close()
+
+
+def _gt_at(scene, i, w, h):
+    gt = scene.views[i].depth
+    if gt.shape[1] == w and gt.shape[0] == h:
+        return gt
+    return cv2.resize(gt, (w, h), interpolation=cv2.INTER_NEAREST)
+
+
+def _gate_pipeline(ctx, scene, scale, seed):
+    """Runs main()'s schedule on the reference build, comparing the CUDA path on every run."""
+    import pipeline as op
+
+    cams = scene_cams(scene)
+    srcs = [[j for j, _ in p] for p in scene.pairs]
+    P = op.OraclePipeline([v.image for v in scene.views], cams, srcs, initial_image_scale=scale, seed=seed)
+    cuda = CudaRunner(ctx)
+    rows, times = {}, {}
+
+    def runner(images, depths, cams_, params, st, run_seed, view_id):
+        mine = copy_state(st)
+        ctx.profile_enable(hpm_b200.PROFILE_TIMING)
+        cuda(images, depths, cams_, params, mine, run_seed, view_id)
+        prof = ctx.profile_read()
+        ctx.profile_enable(0)
+        ms_ref = ref_cuda.run_patchmatch(images, depths, cams_, params, st, run_seed, view_id)
+        W, H = st.W, st.H
+        key = (f"{W}x{H}", MODE_NAMES.get(int(params.mode), str(int(params.mode))))
+        c = gate3.classify(st.planes[..., 3], st.planes[..., :3], mine.planes[..., 3], mine.planes[..., :3],
+                           images[0], cams_[0], _gt_at(scene, view_id, W, H))
+        gate3.add(rows.setdefault(key, {}), c)
+        t = times.setdefault(key, [0.0, 0.0, 0])
+        t[0] += ms_ref
+        t[1] += prof.init_ms + prof.sweep_ms
+        t[2] += 1
+
+    saved = ora.run_patchmatch
+    ora.run_patchmatch = runner
+    try:
+        P.reconstruct(fuse=False)
+    finally:
+        ora.run_patchmatch = saved
+    return rows, times
+
+
+def _report(rows, times, title):
+    text = gate3.table({f"{k[0]} {k[1]}": v for k, v in rows.items()}, title)
+    text += "\n\n| level mode | runs | reference RunPatchMatch ms | CUDA path kernels ms |\n|---|---|---|---|\n"
+    for k, (tr, to, n) in times.items():
+        text += f"| {k[0]} {k[1]} | {n} | {tr:.1f} | {to:.1f} |\n"
+    print("\n" + text)
+    out = os.environ.get("HPM_GATE3_REPORT")
+    if out:
+        with open(out, "a") as fh:
+            fh.write(text + "\n\n")
+    return text
+
+
+def _check(rows):
+    total = {}
+    for c in rows.values():
+        gate3.add(total, c)
+    f = gate3.fractions(total)
+    per_mode = {k: gate3.fractions(c) for k, c in rows.items()}
+    return f, per_mode
+
+
+def test_gate3_c1_every_pass(ctx):
+    """C1: 5 views 1280x960 on a 30-degree arc, --initial-image-scale 4, 4 sources."""
+    from hpm_b200 import synth
+
+    scene = synth.make_scene(n_views=5, width=1280, height=960, layout="arc", n_src=4, seed=11)
+    rows, times = _gate_pipeline(ctx, scene, 4, seed=5)
+    _report(rows, times, "C1 (5 views 1280x960, scale 4 -> 320x240, S = 4): every pass, all views")
+    f, per_mode = _check(rows)
+    assert f["agree"] > 0.80, f
+    assert f["unexplained"] < 0.05, f
+
+
+def test_gate3_1600x1200_s10_every_mode(ctx):
+    """11 views 1600x1200 on the two-ring hemisphere, 10 sources each, --initial-image-scale 1."""
+    from hpm_b200 import synth
+
+    scene = synth.make_scene(n_views=11, width=1600, height=1200, layout="hemisphere", n_src=10, seed=2024,
+                             device="cuda:0")
+    rows, times = _gate_pipeline(ctx, scene, 1, seed=9)
+    _report(rows, times, "11 views 1600x1200, scale 1 (levels 800x600, 1600x1200), S = 10: every pass, all views")
+    f, per_mode = _check(rows)
+    assert f["agree"] > 0.80, f
+    assert f["unexplained"] < 0.05, f
+
+
+def test_cuda_matches_oracle_at_1600x1200_s10(ctx):
+    """Initialisation and the first two half-sweeps (iteration 0, black then red) at the bench's working size
+    with 10 sources: every plane, cost, view mask and draw counter equal to the oracle's bits."""
+    from hpm_b200 import synth
+
+    scene = synth.make_scene(n_views=11, width=1600, height=1200, layout="hemisphere", n_src=10, seed=77,
+                             device="cuda:0")
+    cams = scene_cams(scene)
+    grays = [synth.gray_float(v.image) for v in scene.views]
+    srcs = [j for j, _ in scene.pairs[0]]
+    assert len(srcs) == 10
+    for i, (g, c) in enumerate(zip(grays, cams)):
+        ctx.set_view(i, g, c)
+    canny = cv2.Canny(scene.views[0].image, 50, 150)
+    ctx.set_canny(0, canny)
+    params = hpm_b200.Params.make(len(srcs) + 1, *hpm_b200.widened_range(cams[0]))
+    got = ctx.run_partial(0, srcs, params, 2, seed=123)
+    H, W = grays[0].shape
+    st = ora.RunState(W, H)
+    st.canny[:] = canny
+    imgs = [grays[0]] + [grays[j] for j in srcs]
+    cs = [cams[0]] + [cams[j] for j in srcs]
+    ora.random_init(imgs, cs, params, st, 123, 0)
+    for h in range(2):
+        ora.half_sweep(imgs, None, cs, params, st, h & 1, h >> 1, 123, 0)
+
+    def same(a, b):
+        return bool(((a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))).all())
+
+    assert same(got["planes"], st.planes)
+    assert same(got["costs"], st.costs)
+    assert (got["selected_views"] == st.selected_views).all()
+    assert (got["rng_draw"] == st.rng_draw).all()

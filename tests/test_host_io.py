@@ -121,6 +121,54 @@ def test_jpeg_grey_and_errors(host):
         decode(host, b"GIF89a........")
 
 
+def _segment(data: bytearray, marker: int) -> int:
+    """Offset of the first segment with the given marker byte (0xFF marker)."""
+    return bytes(data).index(bytes([0xFF, marker]))
+
+
+def _corrupt(data: bytes, marker: int, edit) -> bytes:
+    b = bytearray(data)
+    edit(b, _segment(b, marker))
+    return bytes(b)
+
+
+def _set_len(b: bytearray, at: int, length: int) -> None:
+    b[at + 2], b[at + 3] = length >> 8, length & 0xFF
+
+
+def test_jpeg_rejects_corrupt_segments(host):
+    """Malformed table and scan headers are rejected with an error, never read past their segment."""
+    ok, b = cv2.imencode(".jpg", _image(), [cv2.IMWRITE_JPEG_QUALITY, 90])
+    good = b.tobytes()
+    decode(host, good)
+    cases = [
+        # SOS: Huffman table selectors 5 / 7 (only 0..3 exist)
+        (0xDA, lambda b, at: b.__setitem__(at + 6, 0x57), "Huffman table selector"),
+        # SOS: length too short for its component list
+        (0xDA, lambda b, at: _set_len(b, at, 2 + 3), "truncated scan header"),
+        # DHT: length shorter than the 16 code-length counts
+        (0xC4, lambda b, at: _set_len(b, at, 2 + 10), "truncated Huffman table"),
+        # DHT: a code-length count whose symbols run past the segment
+        (0xC4, lambda b, at: b.__setitem__(at + 5 + 15, 200), "Huffman table"),
+        # DQT: precision 2 (only 8- and 16-bit tables exist)
+        (0xDB, lambda b, at: b.__setitem__(at + 4, 0x20 | (b[at + 4] & 15)), "precision"),
+        # DQT: length shorter than one 64-entry table
+        (0xDB, lambda b, at: _set_len(b, at, 2 + 30), "truncated quantisation table"),
+        # SOF: length shorter than the component list
+        (0xC0, lambda b, at: _set_len(b, at, 2 + 8), "truncated frame header"),
+    ]
+    for marker, edit, msg in cases:
+        with pytest.raises(ValueError, match=msg):
+            decode(host, _corrupt(good, marker, edit))
+    # a file cut anywhere in its headers or scan decodes or fails cleanly
+    sos = _segment(bytearray(good), 0xDA)
+    for cut in list(range(2, sos + 16)) + list(range(sos + 16, len(good), 97)):
+        try:
+            decode(host, good[:cut])
+        except ValueError:
+            pass
+
+
 def test_scene_folder_formats(tmp_path):
     """cams, pair.txt and .dmb as the reference reads them, via the command-line driver's own parser."""
     from hpm_b200 import synth
