@@ -78,11 +78,13 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--views", type=int, default=49)
-    ap.add_argument("--width", type=int, default=1600)
-    ap.add_argument("--height", type=int, default=1200)
-    ap.add_argument("--n-src", type=int, default=10)
-    ap.add_argument("--scale", type=int, default=1, help="--initial-image-scale")
+    ap.add_argument("--config", choices=("c1", "c2", "c3", "c4", "c5"), default="c2",
+                    help="workload (synth.CONFIGS); c2, the 49-view 1600x1200 scene, is the headline")
+    ap.add_argument("--views", type=int, default=None, help="override the workload's view count")
+    ap.add_argument("--width", type=int, default=None, help="custom hemisphere scene of this width")
+    ap.add_argument("--height", type=int, default=None)
+    ap.add_argument("--n-src", type=int, default=None)
+    ap.add_argument("--scale", type=int, default=None, help="--initial-image-scale")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chosen-form", action=argparse.BooleanOptionalAction, default=True,
@@ -142,13 +144,47 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ workload
 
+def resolve_workload(args):
+    """Fills args.views/width/height/n_src/scale from --config unless given (width/height: custom scene)."""
+    defaults = {"c1": (5, 1280, 960, 4, 4), "c2": (49, 1600, 1200, 10, 1), "c3": (49, 1600, 1200, 10, 1),
+                "c4": (20, 1024, 768, 10, 1), "c5": (120, 3072, 2048, 10, 1)}
+    v, w, h, ns, sc = defaults[args.config]
+    args.custom = args.width is not None or args.height is not None
+    args.views_given = args.views is not None
+    args.views = args.views or v
+    args.width = args.width or w
+    args.height = args.height or h
+    args.n_src = args.n_src or ns
+    args.scale = args.scale or sc
+
+
 def make_workload(args, device: str, rank: int):
     """The seeded scene of this rank (rendered on the GPU through torch)."""
     import importlib
     _import_pkg()
     synth = importlib.import_module("hpm_b200.synth")
-    return synth.make_scene(n_views=args.views, width=args.width, height=args.height, layout="hemisphere",
-                            n_src=args.n_src, seed=args.seed + 7919 * rank, device=device)
+    if args.custom:
+        return synth.make_scene(n_views=args.views, width=args.width, height=args.height, layout="hemisphere",
+                                n_src=args.n_src, seed=args.seed + 7919 * rank, device=device)
+    return synth.make_config(args.config, seed=args.seed + 7919 * rank, device=device, n_views=args.views)
+
+
+def workload_text(args, scene=None) -> str:
+    if args.custom or args.config in ("c1", "c2", "c4"):
+        desc = (f"{args.views} views {args.width}x{args.height} "
+                f"{'arc' if args.config == 'c1' and not args.custom else 'hemisphere'}, {args.n_src} sources")
+    else:
+        import importlib
+        _import_pkg()
+        desc = importlib.import_module("hpm_b200.synth").CONFIGS[args.config]
+        if args.views_given:
+            desc += f" ({args.views} views)"
+    levels = "/".join(f"{w}x{h}" for w, h in level_sizes(args.width, args.height, args.scale))
+    extra = ""
+    if scene is not None and scene.meta.get("textureless_area"):
+        extra = f", textureless area {scene.meta['textureless_area']:.2f}"
+    return (f"{desc}, --initial-image-scale {args.scale}, levels {levels} (largest view), geometric iterations 3, "
+            f"fusion{extra}")
 
 
 def level_sizes(w: int, h: int, scale: int):
@@ -219,19 +255,19 @@ def run_ours(args, scene, rank, world, local_rank):
         b = pin(v.image.shape, torch.uint8)
         b[...] = v.image
         images.append(b)
-    final_w, final_h = level_sizes(args.width, args.height, args.scale)[-1]
-    depth_out = [pin((final_h, final_w), torch.float32) for _ in range(n_views)]
-    normal_out = [pin((final_h, final_w, 3), torch.float32) for _ in range(n_views)]
+    finals = [level_sizes(v.image.shape[1], v.image.shape[0], args.scale)[-1] for v in scene.views]
+    depth_out = [pin((h, w), torch.float32) for w, h in finals]
+    normal_out = [pin((h, w, 3), torch.float32) for w, h in finals]
     points_out = [None]  # sized after the first step (the point count repeats: same seed, same work)
     h2d_bytes = int(sum(b.nbytes for b in images))
 
-    def step():
+    def step(**recon):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         ev[0].record(stream)
         for i, b in enumerate(images):
             ctx.set_image(i, b)
         ev[1].record(stream)
-        n = ctx.reconstruct(cams, srcs, initial_image_scale=args.scale, seed=args.seed, fuse=True)
+        n = ctx.reconstruct(cams, srcs, initial_image_scale=args.scale, seed=args.seed, fuse=True, **recon)
         ev[2].record(stream)
         if points_out[0] is None or points_out[0].shape[0] < n:
             points_out[0] = pin((n + 4096, 9), torch.float32)
@@ -315,10 +351,7 @@ def run_ours(args, scene, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.views} views {args.width}x{args.height} hemisphere, {args.n_src} sources, "
-                               f"--initial-image-scale {args.scale}, levels "
-                               f"{'/'.join(f'{w}x{h}' for w, h in level_sizes(args.width, args.height, args.scale))}"
-                               f", geometric iterations 3, fusion",
+        "config": {"workload": workload_text(args, scene), "name": args.config,
                    "seed": args.seed, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (several GB of maps per step)",
                    "points_per_step": int(n_pts)},
@@ -328,6 +361,7 @@ def run_ours(args, scene, rank, world, local_rank):
         "roofline": roofline,
         "accuracy": {"measure": "share of ground-truth pixels with depth within 1 %, all views, last step",
                      "plain": accuracy},
+        "stages": stage_breakdown(prof, dev_ms / max(args.steps, 1), n_views, args.steps),
     }
     if args.chosen_form:
         result["chosen_form"] = chosen_form(args, ctx, step, n_views, world, device, depth_out, scene)
@@ -335,30 +369,60 @@ def run_ours(args, scene, rank, world, local_rank):
     return result, ctx, images
 
 
+def stage_breakdown(prof, step_ms: float, n_views: int, steps: int) -> dict:
+    """Device seconds per reference view of each stage of a step (CUDA events around every stage)."""
+    k = 1e-3 / max(steps, 1) / n_views
+    sec = {"patchmatch_gpu": (prof.init_ms + prof.sweep_ms) * k, "confidence": prof.confidence_ms * k,
+           "prior": prof.prior_ms * k, "jbu": prof.jbu_ms * k, "fusion": prof.fusion_ms * k}
+    sec["other"] = max(0.0, step_ms * 1e-3 / n_views - sum(sec.values()))
+    return {"views": n_views, "seconds_per_view": {a: round(b, 5) for a, b in sec.items()}}
+
+
+def agreement(depths, ref_depths, rel: float = 0.005):
+    """Share of pixels (finite, positive reference depth) whose depth is within `rel` of the reference's."""
+    ok = hit = 0
+    for d, r in zip(depths, ref_depths):
+        m = np.isfinite(r) & (r > 0)
+        ok += int(m.sum())
+        with np.errstate(invalid="ignore"):
+            hit += int((np.abs(d[m] - r[m]) <= rel * r[m]).sum())
+    return hit / ok if ok else None
+
+
 def chosen_form(args, ctx, step, n_views, world, device, depth_out=None, scene=None):
-    """The same steps with 8-bit source textures (hpm_set_texture_format(HPM_TEX_U8)), the precision
-    form: the grey levels are stored exactly in a quarter of the bytes, the texture unit returns the
-    filtered sample as grey / 255, and the scale-free NCC only rescales its flat-source test."""
+    """The chosen form of the same steps: 8-bit source textures (hpm_set_texture_format(HPM_TEX_U8): the
+    grey levels stored exactly in a quarter of the bytes, the filtered sample returned as grey / 255, the
+    scale-free NCC only rescaling its flat-source test), every pass batched where that leaves the result
+    unchanged (hpm_run_batch: one launch per stage over all views, autotuned launch shape) and the batched
+    schedules replayed from CUDA graphs.  Also timed: the same with the multi-geometry passes batched too
+    (Jacobi), a change of iteration that is reported with its agreement."""
     import torch
     hb = _import_pkg()
+    plain = [d.copy() for d in depth_out] if depth_out is not None else None
+    out = {"form": "8-bit source textures + batched passes (exact) + CUDA-graph replay", "unit": UNIT}
     ctx.set_texture_format(hb.TEX_U8)
-    for _ in range(max(1, min(args.warmup, 2))):
-        step()
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    evs = [step()[0] for _ in range(args.steps)]
-    torch.cuda.synchronize()
-    accuracy = depth_accuracy(depth_out, scene) if depth_out is not None and scene is not None else None
+    ctx.set_batch_options(hb.BATCH_AUTOTUNE | hb.BATCH_GRAPH)
+    for name, batch in (("", hb.RECON_BATCH_EXACT), ("jacobi_", hb.RECON_BATCH_ALL)):
+        for _ in range(max(1, min(args.warmup, 2))):
+            step(batch=batch)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        evs = [step(batch=batch)[0] for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        dev_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
+        e2e_ms = sum(e[0].elapsed_time(e[3]) for e in evs)
+        t = max_over_ranks([dev_ms, e2e_ms], world, device)
+        total_views = n_views * args.steps * world
+        out[name + "value"] = total_views / (float(t[0]) / 1e3)
+        out[name + "e2e"] = total_views / (float(t[1]) / 1e3)
+        out[name + "ms_per_step"] = float(t[0]) / args.steps
+        if depth_out is not None and scene is not None:
+            out[name + "accuracy"] = depth_accuracy(depth_out, scene)
+            out[name + "agree_with_plain_0p5pct"] = agreement(depth_out, plain)
     ctx.set_texture_format(hb.TEX_F32)
-    dev_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
-    e2e_ms = sum(e[0].elapsed_time(e[3]) for e in evs)
-    t = max_over_ranks([dev_ms, e2e_ms], world, device)
-    total_views = n_views * args.steps * world
-    return {"form": "8-bit source textures (cost error against the FP64 exact-bilinear cost as for float "
-                    "textures; same accuracy against the rendered ground truth, tests/test_gpu_texf16.py)",
-            "value": total_views / (float(t[0]) / 1e3), "e2e": total_views / (float(t[1]) / 1e3),
-            "unit": UNIT, "ms_per_step": float(t[0]) / args.steps, "accuracy": accuracy}
+    ctx.set_batch_options(hb.BATCH_AUTOTUNE)
+    return out
 
 
 def max_over_ranks(values, world: int, device):
@@ -431,7 +495,7 @@ def cpu_port_baseline(args, scene):
     dt = time.perf_counter() - t0
     px_runs = 2 * sw * sh
     rate = px_runs / dt
-    per_view = view_pixel_runs(args.width, args.height, args.scale)
+    per_view = int(np.mean([view_pixel_runs(v.image.shape[1], v.image.shape[0], args.scale) for v in scene.views]))
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return {"value": rate / per_view, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"oracle C port (OpenMP), one photometric + one geometric PatchMatch run of one view at "
@@ -442,238 +506,74 @@ def cpu_port_baseline(args, scene):
 
 # ------------------------------------------------------------------ reference arm
 
-REF_HOST_LIB = os.path.join(ORACLE, "_ref", "libhpmref_host.so")
-
-
-def time_reference_host_stages(L, srcs, folder):
-    """The reference's own ConfidenceEvaluation and RunFusion (main.cpp, compiled from its sources by
-    oracle/ref_host.mk) on one level's maps: the dense folder they read is written first (not timed), then
-    each stage is timed as the reference runs it, reading its inputs from the folder.  Returns
-    (confidence seconds, fusion seconds)."""
-    import ctypes
-    n = len(L["depth"])
-    for sub_dir in ("cams", "images"):
-        os.makedirs(os.path.join(folder, sub_dir), exist_ok=True)
-    for i in range(n):
-        c = L["cams"][i]
-        K, R, t = np.array(c.K).reshape(3, 3), np.array(c.R).reshape(3, 3), np.array(c.t)
-        with open(os.path.join(folder, "cams", f"{i:08d}_cam.txt"), "w") as fh:
-            fh.write("extrinsic\n")
-            for r in range(3):
-                fh.write(" ".join(f"{R[r, k]:.9g}" for k in range(3)) + f" {t[r]:.9g}\n")
-            fh.write("0 0 0 1\n\nintrinsic\n")
-            for r in range(3):
-                fh.write(" ".join(f"{K[r, k]:.9g}" for k in range(3)) + "\n")
-            fh.write(f"\n{c.depth_min:.9g} 0.01 192 {c.depth_max:.9g}\n")
-        img = np.ascontiguousarray(L["imgs"][i], np.uint8)
-        with open(os.path.join(folder, "images", f"{i:08d}.jpg.raw"), "wb") as fh:
-            fh.write(np.array([img.shape[0], img.shape[1], 3], np.int32).tobytes())
-            fh.write(img.tobytes())
-        res = os.path.join(folder, "HPM_MVS_plusplus", f"2333_{i:08d}")
-        os.makedirs(res, exist_ok=True)
-        for name, a in (("depths.dmb", L["depth"][i]), ("normals.dmb", L["normal"][i])):
-            a = np.ascontiguousarray(a, np.float32)
-            with open(os.path.join(res, name), "wb") as fh:
-                fh.write(np.array([1, a.shape[0], a.shape[1], 1 if a.ndim == 2 else a.shape[2]], np.int32).tobytes())
-                fh.write(a.tobytes())
-        # the geometric maps are the same maps here: a second name for the same file
-        try:
-            os.link(os.path.join(res, "depths.dmb"), os.path.join(res, "depths_geom.dmb"))
-        except OSError:
-            import shutil
-            shutil.copyfile(os.path.join(res, "depths.dmb"), os.path.join(res, "depths_geom.dmb"))
-    off = np.zeros(n + 1, np.int32)
-    for i, sl in enumerate(srcs):
-        off[i + 1] = off[i] + len(sl)
-    ids = np.concatenate([np.asarray(sl, np.int32) for sl in srcs])
-    lib = ctypes.CDLL(REF_HOST_LIB)
-    vp = ctypes.c_void_p
-    lib.ref_host_confidence.argtypes = [ctypes.c_char_p, ctypes.c_int, vp, vp, ctypes.c_int]
-    lib.ref_host_fusion.argtypes = [ctypes.c_char_p, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int]
-    t0 = time.perf_counter()
-    rc = lib.ref_host_confidence(folder.encode(), n, off.ctypes.data, ids.ctypes.data, 0)
-    conf_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    rc |= lib.ref_host_fusion(folder.encode(), n, off.ctypes.data, ids.ctypes.data, 1, 0)
-    fusion_s = time.perf_counter() - t0
-    if rc != 0:
-        raise RuntimeError("reference host stages failed")
-    return conf_s, fusion_s
-
 def run_reference(args):
-    """The reference's own implementation of the path, one sampled reference view per step: its PatchMatch
-    runs through the reference's CUDA kernels (HPM.cu built from its sources, oracle/_ref), the per-run host
-    work it does (grey conversion of all views, Canny), its host prior construction (support points,
-    cv::Subdiv2D, raster and plane fits) and a per-view share of its single-threaded ConfidenceEvaluation and
-    RunFusion scans, timed on this box."""
-    ora = _import_oracle()
+    """The reference's own implementation of the path, like for like: the whole schedule of its main() on
+    one reference view and its sources (every view keeping the workload's size and source count), on the
+    reference's own code where it was built here (oracle/ref_pipeline.py): HPM::RunPatchMatch of its HPM.cu
+    compiled for sm_100a, its JBU kernel, its single-threaded ConfidenceEvaluation and RunFusion compiled
+    for the CPU, its prior construction (cv2.Subdiv2D plus the C restatement of its raster and fits).  Each
+    pass takes its inputs from the reference's own earlier passes.  That reconstruction is timed stage by
+    stage; each step then replays the first view's share of it (its runs from their recorded inputs, its
+    prior construction, 1/N of the whole-scene host stages)."""
+    _import_oracle()
     import ref_cuda  # noqa: E402  (oracle/ref_cuda.py)
-    import cv2
+    import ref_pipeline  # noqa: E402  (oracle/ref_pipeline.py)
     if not ref_cuda.available():
         return {"impl": "reference", "unavailable": "reference CUDA build oracle/_ref/libhpmref.so was not built"}
     hb = _import_pkg()
     import torch
     torch.cuda.set_device(0)
     scene = make_workload(args, "cuda:0", 0)
-    sizes = level_sizes(args.width, args.height, args.scale)
-    n_views = len(scene.views)
-    srcs = [[j for j, _ in p] for p in scene.pairs]
-    base_cams = [ora.to_cam(hb.Camera.make(v.K, v.R, v.t, v.image.shape[1], v.image.shape[0], v.depth_min,
-                                           v.depth_max)) for v in scene.views]
-
-    def level_cam(i, w, h):
-        c = ora.to_cam(base_cams[i])
-        sx, sy = np.float32(w) / np.float32(c.width), np.float32(h) / np.float32(c.height)
-        c.K[0] = float(np.float32(c.K[0]) * sx); c.K[2] = float(np.float32(c.K[2]) * sx)
-        c.K[4] = float(np.float32(c.K[4]) * sy); c.K[5] = float(np.float32(c.K[5]) * sy)
-        c.width, c.height = w, h
-        return c
-
-    # level images (PrepareScaleImages runs once per level for all views; its per-view share is timed below)
-    levels = []
-    for (w, h) in sizes:
-        imgs = [cv2.resize(v.image, (w, h), interpolation=cv2.INTER_LINEAR) if (w, h) != v.image.shape[1::-1]
-                else v.image for v in scene.views]
-        gt_d = [cv2.resize(v.depth, (w, h), interpolation=cv2.INTER_NEAREST) for v in scene.views]
-        gt_n = [cv2.resize(v.normal.astype(np.float32), (w, h), interpolation=cv2.INTER_NEAREST)
-                for v in scene.views]
-        levels.append({"w": w, "h": h, "imgs": imgs, "cams": [level_cam(i, w, h) for i in range(n_views)],
-                       "depth": gt_d, "normal": gt_n})
-    # the whole-scene host scans, timed once per level on the box and shared per view: the reference's own
-    # ConfidenceEvaluation and RunFusion where their CPU build is present, else their C restatement
-    scan_s, fusion_s, scans_from = [], 0.0, "their C restatement"
+    v0 = 0
+    subset = [v0] + [j for j, _ in scene.pairs[v0]]
+    score = lambda g, j: dict(scene.pairs[g]).get(j, -1.0)  # noqa: E731
+    # every view of the subset keeps its source count: the other subset views by its pair.txt score
+    srcs = [sorted([k for k in range(len(subset)) if k != a], key=lambda k: -score(subset[a], subset[k]))
+            [:len(scene.pairs[g])] for a, g in enumerate(subset)]
+    cams = [hb.Camera.make(scene.views[g].K, scene.views[g].R, scene.views[g].t, scene.views[g].image.shape[1],
+                           scene.views[g].image.shape[0], scene.views[g].depth_min, scene.views[g].depth_max)
+            for g in subset]
+    folder = tempfile.mkdtemp(prefix="hpm_ref_")
+    P = ref_pipeline.RefPipeline([scene.views[g].image for g in subset], cams, srcs,
+                                 initial_image_scale=args.scale, seed=args.seed, record_view=0, folder=folder)
     try:
-        import shutil
-        if not os.path.exists(REF_HOST_LIB):
-            raise FileNotFoundError(REF_HOST_LIB)
-        for li, L in enumerate(levels):
-            folder = tempfile.mkdtemp(prefix="hpm_ref_host_")
-            try:
-                conf_s, fus_s = time_reference_host_stages(L, srcs, folder)
-            finally:
-                shutil.rmtree(folder, ignore_errors=True)
-            scan_s.append(conf_s)
-            if li == len(levels) - 1:
-                fusion_s = fus_s
-        scans_from = "the reference's own main.cpp (oracle/_ref/libhpmref_host.so), .dmb reads included"
-    except Exception as e:  # the restatement stands in, and the line says so
-        print(f"reference host stages unavailable ({e}); timing their C restatement", file=sys.stderr)
-        scan_s = []
-        for L in levels:
-            t0 = time.perf_counter()
-            ora.confidence_eval(L["cams"], L["depth"], L["normal"], srcs)
-            scan_s.append(time.perf_counter() - t0)
-        L = levels[-1]
         t0 = time.perf_counter()
-        ora.fusion(L["cams"], L["depth"], L["normal"], L["imgs"], srcs)
-        fusion_s = time.perf_counter() - t0
-
-    def one_view(v):
-        t_total = 0.0
-        n_levels = len(levels)
-        for li, L in enumerate(levels):
-            level = n_levels - 1 - li
-            w, h = L["w"], L["h"]
-            ids = [v] + srcs[v]
-            cams = [L["cams"][j] for j in ids]
-            dmin = float(np.float32(cams[0].depth_min) * np.float32(0.6))
-            dmax = float(np.float32(cams[0].depth_max) * np.float32(1.2))
-            gt_conf = (L["depth"][v] > 0).astype(np.float32) * np.float32(0.5)
-
-            def pm(mode, prior=None):
-                t0 = time.perf_counter()
-                # per-run host work of ProcessProblem/InuputInitialization (main.cpp:237-330, HPM.cpp:643-697)
-                grays = [cv2.cvtColor(L["imgs"][j], cv2.COLOR_BGR2GRAY).astype(np.float32) for j in ids]
-                edges = cv2.Canny(L["imgs"][v], 50, 150)
-                p = ora.Params()
-                p.max_iterations, p.patch_size, p.num_images, p.radius_increment = 3, 11, len(ids), 2
-                p.sigma_spatial, p.sigma_color, p.top_k = 5.0, 3.0, 4
-                p.depth_min, p.depth_max = dmin, dmax
-                p.mode = mode
-                st = ora.RunState(w, h)
-                st.canny[:] = edges
-                st.planes[..., :3] = L["normal"][v]
-                st.planes[..., 3] = L["depth"][v]
-                st.costs[:] = 0.5
-                st.confidences[:] = gt_conf
-                if prior is not None:
-                    st.prior_planes[:], st.plane_masks[:] = prior
-                depths = None
-                if mode & 1:
-                    depths = [None] + [L["depth"][j] for j in srcs[v]]
-                if mode & 8:
-                    prev = levels[li - 1]
-                    sp = np.zeros((prev["h"], prev["w"], 4), np.float32)
-                    sp[..., :3] = prev["normal"][v]
-                    sp[..., 3] = 0.5
-                    st.scaled_planes = sp
-                    p.scaled_cols, p.scaled_rows = prev["w"], prev["h"]
-                    p.mode |= 16
-                ref_cuda.run_patchmatch(grays, depths, cams, p, st, 17, v)
-                return time.perf_counter() - t0
-
-            def build_prior(distance):
-                t0 = time.perf_counter()
-                import pipeline as op
-                cost = np.full((h, w), 0.05, np.float32)
-                if distance == 0:
-                    pts = ora.support_points(cost, gt_conf, w, h)
-                    tris = op.cv2_triangles(pts, w, h)
-                    label, fits, _, _ = ora.planar_prior(tris, L["depth"][v], cams[0], 1.0, dmin, dmax, 0)
-                    lab = label.astype(np.int64)
-                    prior = np.zeros((h, w, 4), np.float32)
-                    prior[lab > 0] = fits[lab[lab > 0] - 1]
-                    mask = (lab > 0).astype(np.uint32)
-                else:
-                    f = np.float32(1.0) / np.float32(distance * 2)
-                    hw, hh = int(round(float(np.float32(w) * f))), int(round(float(np.float32(h) * f)))
-                    dd = ora.resize_linear(L["depth"][v], hw, hh)
-                    pts = ora.support_points(ora.resize_linear(cost, hw, hh), ora.resize_linear(gt_conf, hw, hh),
-                                             int(np.float32(w) * f), int(np.float32(h) * f))
-                    tris = op.cv2_triangles(pts, hw, hh)
-                    _, _, pdepth, pnormal = ora.planar_prior(tris, dd, cams[0], float(f), dmin, dmax, 1)
-                    ud = cv2.resize(pdepth, (w, h))
-                    un = cv2.resize(pnormal, (w, h))
-                    prior, m8 = ora.prior_reload(ud, un, cams[0], dmin, dmax)
-                    mask = m8.astype(np.uint32)
-                return (prior, mask), time.perf_counter() - t0
-
-            t_total += pm(8 if li > 0 else 0)
-            for hpm_scale in range(n_levels - 1, level - 1, -1):
-                t_total += scan_s[li] / n_views
-                distance = hpm_scale - level
-                prior, tp = build_prior(min(distance, 2))
-                t_total += tp + pm(2, prior)
-            for it in range(3):
-                mode = 1
-                if it > 0:
-                    mode |= 4 | 32
-                    t_total += scan_s[li] / n_views
-                t_total += pm(mode)
-        return t_total + fusion_s / n_views
-
-    for s in range(max(args.warmup, 0)):
-        one_view(s % n_views)
-    times = [one_view((args.warmup + s) % n_views) for s in range(args.steps)]
+        P.reconstruct(fuse=True)
+        whole_s = time.perf_counter() - t0
+        n = len(subset)
+        for _ in range(max(args.warmup, 0)):
+            P.replay(1.0 / n)
+        times = [P.replay(1.0 / n) for _ in range(args.steps)]
+    finally:
+        P.close()
     total = sum(times)
     value = args.steps / total
-    threads = 1
+    pm_ms = {f"{k[0]} {k[1]}": round(v[0] / v[1], 2) for k, v in P.pm.items()}
+    pm_s = sum(v[0] for v in P.pm.values()) / 1e3
+    stage_s = {"patchmatch_gpu": pm_s, "patchmatch_host": P.t["pm_host_s"], "prior": P.t["prior_s"],
+               "confidence": P.t["confidence_s"], "jbu": P.t["jbu_s"], "fusion": P.t["fusion_s"]}
+    host_from = ("the reference's own main.cpp (oracle/_ref/libhpmref_host.so)" if P.host is not None
+                 else "their C restatement (the reference's host build is absent)")
     result = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.views} views {args.width}x{args.height} hemisphere, {args.n_src} sources, "
-                               f"--initial-image-scale {args.scale}, levels "
-                               f"{'/'.join(f'{w}x{h}' for w, h in sizes)}, geometric iterations 3, fusion",
-                   "seed": args.seed, "step": "one sampled reference view through the whole schedule"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": "per step one reference view: the reference's PatchMatch runs on its own CUDA "
-                                   "kernels (HPM.cu compiled for sm_100a, fast-math as shipped), its per-run host "
-                                   "work (grey conversion, Canny), host prior construction (cv2.Subdiv2D and the "
-                                   "C restatement of its raster and fits), and 1/N of its single-threaded "
-                                   f"ConfidenceEvaluation ({', '.join(f'{t:.1f}' for t in scan_s)} s per level) "
-                                   f"and RunFusion ({fusion_s:.1f} s) scans, timed on {scans_from}; inputs of "
-                                   "the later passes from the rendered ground truth; JBU and image IO not timed"},
+        "config": {"workload": workload_text(args), "name": args.config, "seed": args.seed,
+                   "step": f"view 0's share of the reference's whole schedule over view 0 and its {n - 1} sources"},
+        "stages": {"views": n, "seconds": {k: round(v, 3) for k, v in stage_s.items()},
+                   "seconds_per_view": {k: round(v / n, 5) for k, v in stage_s.items()},
+                   "reconstruct_wall_s": round(whole_s, 2), "views_per_s_whole": n / sum(stage_s.values()),
+                   "patchmatch_ms_per_run": pm_ms, "host_cores": 1,
+                   "host_stages_from": host_from},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": "per step one reference view: its PatchMatch runs on the reference's own CUDA "
+                                   "kernels (HPM.cu compiled for sm_100a, fast-math as shipped) from the inputs its "
+                                   "own earlier passes produced, its per-run host work (grey conversion, Canny), "
+                                   "its prior construction (cv2.Subdiv2D and the C restatement of its raster and "
+                                   f"fits), and 1/{n} of the single-threaded ConfidenceEvaluation "
+                                   f"({P.t['confidence_s']:.1f} s), RunFusion ({P.t['fusion_s']:.1f} s) and JBU "
+                                   f"({P.t['jbu_s']:.2f} s) of that {n}-view reconstruction, timed on {host_from}, "
+                                   ".dmb reads included; file writes and image decoding not timed"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return result
@@ -683,6 +583,7 @@ def run_reference(args):
 
 def main():
     args = parse_args()
+    resolve_workload(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

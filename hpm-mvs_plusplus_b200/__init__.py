@@ -44,8 +44,15 @@ EXPORTED_SYMBOLS = (
     "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior", "hpm_set_image", "hpm_prepare_level",
     "hpm_get_level", "hpm_reconstruct", "hpm_get_points", "hpm_get_stream", "hpm_profile_enable",
     "hpm_profile_read", "hpm_measure_fp32_peak", "hpm_eval_costs_noalloc", "hpm_eval_cost_grad", "hpm_gn_refine",
-    "hpm_set_texture_format",
+    "hpm_set_texture_format", "hpm_run_batch", "hpm_set_batch_options",
 )
+
+BATCH_AUTOTUNE = 1
+BATCH_GRAPH = 2
+
+RECON_SEQUENTIAL = 0
+RECON_BATCH_EXACT = 1
+RECON_BATCH_ALL = 2
 
 TEX_F32 = 0
 TEX_F16 = 1
@@ -60,14 +67,17 @@ class Profile(ctypes.Structure):
 
     _fields_ = [("init_launches", ctypes.c_int64), ("sweep_launches", ctypes.c_int64),
                 ("init_ms", ctypes.c_double), ("sweep_ms", ctypes.c_double),
-                ("init_view_evals", ctypes.c_uint64), ("sweep_view_evals", ctypes.c_uint64)]
+                ("init_view_evals", ctypes.c_uint64), ("sweep_view_evals", ctypes.c_uint64),
+                ("confidence_ms", ctypes.c_double), ("prior_ms", ctypes.c_double), ("jbu_ms", ctypes.c_double),
+                ("fusion_ms", ctypes.c_double)]
 
 
 class ReconOptions(ctypes.Structure):
     """hpm_recon_options: --initial-image-scale, geometric iterations, fusion, seed."""
 
     _fields_ = [("initial_image_scale", ctypes.c_int32), ("geom_iterations", ctypes.c_int32),
-                ("fuse", ctypes.c_int32), ("level_max_side", ctypes.c_int32), ("seed", ctypes.c_uint64)]
+                ("fuse", ctypes.c_int32), ("level_max_side", ctypes.c_int32), ("batch", ctypes.c_int32),
+                ("batch_views", ctypes.c_int32), ("seed", ctypes.c_uint64)]
 
 
 class Point(ctypes.Structure):
@@ -188,6 +198,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                        ctypes.c_uint64]
     lib.hpm_eval_costs.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int, vp, vp,
                                    vp]
+    lib.hpm_run_batch.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, ctypes.c_int, vp]
+    lib.hpm_set_batch_options.argtypes = [vp, ctypes.c_int]
     lib.hpm_eval_costs_noalloc.argtypes = lib.hpm_eval_costs.argtypes
     lib.hpm_eval_cost_grad.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int, vp,
                                        vp, vp, vp]
@@ -328,6 +340,21 @@ class Context:
         s = np.ascontiguousarray(srcs, dtype=np.int32)
         self._check(self.lib.hpm_run_patchmatch(self.h, ref, _ptr(s), len(s), ctypes.byref(params), texture_level,
                                                 ctypes.c_uint64(seed)), "hpm_run_patchmatch")
+
+    def run_batch(self, refs: Sequence[int], src_lists, params, seeds: Sequence[int], texture_level: int = 0) -> None:
+        """hpm_run_batch: the runs (refs[k], src_lists[k], params[k], seeds[k]) in one launch per stage."""
+        n = len(refs)
+        r = np.ascontiguousarray(refs, dtype=np.int32)
+        off, ids = self._src_lists(src_lists)
+        if isinstance(params, Params):
+            params = [params] * n
+        parr = (Params * n)(*params)
+        sd = np.ascontiguousarray(seeds, dtype=np.uint64)
+        self._check(self.lib.hpm_run_batch(self.h, n, _ptr(r), _ptr(off), _ptr(ids), parr, texture_level, _ptr(sd)),
+                    "hpm_run_batch")
+
+    def set_batch_options(self, flags: int) -> None:
+        self._check(self.lib.hpm_set_batch_options(self.h, flags), "hpm_set_batch_options")
 
     def eval_costs(self, ref: int, srcs: Sequence[int], params: Params, px: np.ndarray,
                    planes: np.ndarray) -> np.ndarray:
@@ -490,10 +517,13 @@ class Context:
         return bgr, gray, edges
 
     def reconstruct(self, cams, src_lists, initial_image_scale: int = 4, seed: int = 0, fuse: bool = True,
-                    geom_iterations: int = 3, level_max_side: int = 0) -> int:
+                    geom_iterations: int = 3, level_max_side: int = 0, batch: int = RECON_SEQUENTIAL,
+                    batch_views: int = 0) -> int:
+        """hpm_reconstruct; batch = RECON_SEQUENTIAL / RECON_BATCH_EXACT / RECON_BATCH_ALL (batching form)."""
         cam_arr = (Camera * len(cams))(*cams)
         off, ids = self._src_lists(src_lists)
-        opt = ReconOptions(initial_image_scale, geom_iterations, 1 if fuse else 0, level_max_side, seed)
+        opt = ReconOptions(initial_image_scale, geom_iterations, 1 if fuse else 0, level_max_side, batch,
+                           batch_views, seed)
         n = ctypes.c_int64()
         self._check(self.lib.hpm_reconstruct(self.h, len(cams), cam_arr, _ptr(off), _ptr(ids), ctypes.byref(opt),
                                              ctypes.byref(n)), "hpm_reconstruct")

@@ -79,6 +79,13 @@ Ctx::~Ctx() {
         if (v.color) cudaFree(v.color);
         if (v.orig) cudaFree(v.orig);
     }
+    for (auto& g : batch_graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (void* p : { (void*)b_planes, (void*)b_costs, (void*)b_pre, (void*)b_sel, (void*)b_rng, (void*)b_conf,
+                     (void*)b_scaled, (void*)d_bargs, (void*)d_btiles })
+        if (p) cudaFree(p);
+    if (h_bargs) cudaFreeHost(h_bargs);
+    if (h_btiles) cudaFreeHost(h_btiles);
     for (void* p : { (void*)planes, (void*)costs, (void*)pre_costs, (void*)sel, (void*)rng, (void*)conf,
                      (void*)scaled, (void*)scratch, (void*)scan_state, (void*)scan_work, (void*)points,
                      (void*)prior_small, (void*)prior_tris, (void*)prior_label, (void*)prior_work,
@@ -279,6 +286,21 @@ int hpm_run_patchmatch(hpm_ctx* ctx, int ref, const int32_t* srcs, int n_src, co
     if (!ctx) return HPM_E_INVALID;
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
     return c->run_patchmatch(ref, srcs, n_src, params, texture_level, seed);
+}
+
+int hpm_run_batch(hpm_ctx* ctx, int n, const int32_t* refs, const int32_t* src_off, const int32_t* src_ids,
+                  const hpm_params* params, int texture_level, const uint64_t* seeds) {
+    if (!ctx) return HPM_E_INVALID;
+    return reinterpret_cast<Ctx*>(ctx)->run_batch(n, refs, src_off, src_ids, params, texture_level, seeds);
+}
+
+int hpm_set_batch_options(hpm_ctx* ctx, int flags) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (flags & ~(HPM_BATCH_AUTOTUNE | HPM_BATCH_GRAPH))
+        return c->fail(HPM_E_INVALID, "hpm_set_batch_options: unknown flags 0x%x", flags);
+    c->batch_flags = flags;
+    return HPM_OK;
 }
 
 int hpm_eval_costs(hpm_ctx* ctx, int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n,

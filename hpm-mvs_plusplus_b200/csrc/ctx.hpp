@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "hpm_capi.h"
@@ -12,6 +13,10 @@
 namespace hpm {
 
 constexpr int kNumMaps = 16;
+
+// Kinds of the profiling events (hpm_profile): PatchMatch launches and the other stages of hpm_reconstruct.
+enum { HPM_STAGE_INIT = 0, HPM_STAGE_SWEEP = 1, HPM_STAGE_CONFIDENCE = 2, HPM_STAGE_PRIOR = 3, HPM_STAGE_JBU = 4,
+       HPM_STAGE_FUSION = 5 };
 
 struct DevMap {
     float* ptr = nullptr;
@@ -47,6 +52,26 @@ struct ViewState {
 
 struct SrcImages;
 
+// Device buffers of one PatchMatch run: the context's own (single runs) or one
+// run's slices of the batch buffers (hpm_run_batch).  scaled == nullptr: the
+// hierarchy input goes to the context's own `scaled` buffer.
+struct RunBufs {
+    float4* planes = nullptr;
+    float* costs = nullptr;
+    float* pre_costs = nullptr;
+    uint32_t* sel = nullptr;
+    uint32_t* rng = nullptr;
+    float* conf = nullptr;
+    float4* scaled = nullptr;
+};
+
+// One tuned launch shape of the batched half-sweep (the autotuner's choice).
+struct BatchShape {
+    int bx = 32;       // block width in pixels (block height = block threads / bx row pairs)
+    int persist = 0;   // 0: one block per tile; k > 0: a persistent grid of k x resident blocks
+    float ms = 0.0f;   // measured time of one half-sweep with this shape
+};
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -79,6 +104,28 @@ struct Ctx {
     uint8_t* canny_state = nullptr; size_t canny_state_cap = 0;
     int64_t n_points = 0;
 
+    // batching form (hpm_run_batch): per-run slices of these buffers, the runs'
+    // RunArgs and tile prefix sums in device memory, and the tuned shapes
+    float4* b_planes = nullptr; size_t b_cap_planes = 0;
+    float* b_costs = nullptr; size_t b_cap_costs = 0;
+    float* b_pre = nullptr; size_t b_cap_pre = 0;
+    uint32_t* b_sel = nullptr; size_t b_cap_sel = 0;
+    uint32_t* b_rng = nullptr; size_t b_cap_rng = 0;
+    float* b_conf = nullptr; size_t b_cap_conf = 0;
+    float4* b_scaled = nullptr; size_t b_cap_scaled = 0;
+    RunArgs* d_bargs = nullptr; size_t d_bargs_cap = 0;
+    int* d_btiles = nullptr; size_t d_btiles_cap = 0;    // init tiles (n+1), then sweep tiles (n+1)
+    RunArgs* h_bargs = nullptr; size_t h_bargs_cap = 0;  // pinned staging of the RunArgs
+    int* h_btiles = nullptr; size_t h_btiles_cap = 0;
+    int batch_flags = HPM_BATCH_AUTOTUNE;
+    std::vector<std::pair<uint64_t, BatchShape>> batch_shapes;  // autotuner cache: key -> shape
+    struct BatchGraph {
+        int n = 0, init_tiles = 0, sweep_tiles = 0, max_s = 0, iters = 0, bx = 0, grid = 0;
+        bool mand = false;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::vector<BatchGraph> batch_graphs;
+
     // profiling (hpm_profile_enable): CUDA events around every PatchMatch
     // kernel launch, read back and summed by hpm_profile_read
     int prof_flags = 0;
@@ -98,6 +145,12 @@ struct Ctx {
     int fill_run_args(int ref, const int32_t* srcs, int n_src, const hpm_params* params, RunArgs& a);
     int prepare_run(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int texture_level,
                     uint64_t seed, RunArgs& a);
+    int prepare_run_into(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int texture_level,
+                         uint64_t seed, const RunBufs& b, RunArgs& a);
+    int finish_run(int ref, const RunArgs& a, bool geom);
+    int run_batch(int n, const int32_t* refs, const int32_t* src_off, const int32_t* src_ids,
+                  const hpm_params* params, int texture_level, const uint64_t* seeds);
+    int tune_batch(const BatchLaunch& bl, int n, size_t total_px, uint64_t key, BatchShape& out);
     int launch_schedule(const RunArgs& a, int n_half_sweeps);
     int debug_run_partial(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int texture_level,
                           uint64_t seed, int n_half_sweeps, float* planes_out, float* costs_out, uint32_t* sel_out,

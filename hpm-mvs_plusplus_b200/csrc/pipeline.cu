@@ -49,7 +49,9 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
     int pass = 0;
     int rc = HPM_OK;
 
-    auto run = [&](int i, uint32_t mode, int texture_level) -> int {
+    if (opt->batch < HPM_RECON_SEQUENTIAL || opt->batch > HPM_RECON_BATCH_ALL || opt->batch_views < 0)
+        return fail(HPM_E_INVALID, "hpm_reconstruct: bad batch options");
+    auto make_params = [&](int i, uint32_t mode) -> hpm_params {
         const hpm_camera& c = views[i].cam;
         hpm_params p;
         p.max_iterations = 3;  // RunPatchMatch hard-codes 3 (HPM.cu:3013)
@@ -64,11 +66,53 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
         p.scaled_cols = 0;
         p.scaled_rows = 0;
         p.mode = mode;
+        return p;
+    };
+    auto run = [&](int i, uint32_t mode, int texture_level) -> int {
+        const hpm_params p = make_params(i, mode);
         return run_patchmatch(i, src_ids + src_off[i], p.num_images - 1, &p, texture_level,
                               hpm_run_seed(opt->seed, (uint64_t)pass, (uint64_t)i));
     };
+    // views [first, last) of a pass in one hpm_run_batch: same seeds and inputs as their single runs
+    auto run_group = [&](int first, int last, uint32_t mode, int texture_level) -> int {
+        std::vector<int32_t> refs, off(1, 0), ids;
+        std::vector<hpm_params> prm;
+        std::vector<uint64_t> seeds;
+        for (int i = first; i < last; ++i) {
+            refs.push_back(i);
+            ids.insert(ids.end(), src_ids + src_off[i], src_ids + src_off[i + 1]);
+            off.push_back((int32_t)ids.size());
+            prm.push_back(make_params(i, mode));
+            seeds.push_back(hpm_run_seed(opt->seed, (uint64_t)pass, (uint64_t)i));
+        }
+        return run_batch((int)refs.size(), refs.data(), off.data(), ids.data(), prm.data(), texture_level,
+                         seeds.data());
+    };
+    // a whole pass: batched when the options allow it for this mode, else view by view in order
+    const int group = opt->batch_views > 0 ? opt->batch_views : n_views;
+    auto run_pass = [&](uint32_t mode, int texture_level) -> int {
+        const bool jacobi = mode & HPM_MODE_MULTIGEOM;  // reads depths_geom maps the same pass writes
+        const bool batched = opt->batch == HPM_RECON_BATCH_ALL || (opt->batch == HPM_RECON_BATCH_EXACT && !jacobi);
+        for (int i = 0; i < n_views; i += batched ? group : 1) {
+            const int r = batched ? run_group(i, std::min(n_views, i + group), mode, texture_level)
+                                  : run(i, mode, texture_level);
+            if (r) return r;
+        }
+        return HPM_OK;
+    };
+    // device time of the non-PatchMatch stages, when profiling is on (hpm_profile)
+    auto timed = [&](int kind, auto&& fn) -> int {
+        TimedLaunch* t = nullptr;
+        int r = record_start(kind, t);
+        if (r) return r;
+        r = fn();
+        if (t) cudaEventRecord(t->stop, stream);
+        return r;
+    };
     auto confidence = [&](int depth_kind) -> int {
-        return consistency_scan(0, n_views, src_off, src_ids, depth_kind, nullptr, nullptr, 0, nullptr, nullptr);
+        return timed(HPM_STAGE_CONFIDENCE, [&]() {
+            return consistency_scan(0, n_views, src_off, src_ids, depth_kind, nullptr, nullptr, 0, nullptr, nullptr);
+        });
     };
     // A view's prior depends only on its own maps and the confidences computed
     // before the pass, so all support points are taken first and the host
@@ -87,7 +131,7 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
                 if (dist[i] < 0 || dist[i] > 2)
                     return fail(HPM_E_STATE, "view %d: prior scale distance %d is outside 0..2", i, dist[i]);
                 if (!views[i].maps[HPM_MAP_DEPTH].ptr) return fail(HPM_E_STATE, "view %d lacks a depth map", i);
-                r = support_points(i, dist[i], xy[i], sup_w[i], sup_h[i]);
+                r = timed(HPM_STAGE_PRIOR, [&]() { return support_points(i, dist[i], xy[i], sup_w[i], sup_h[i]); });
                 if (r) return r;
             }
             std::vector<std::future<std::vector<hpm_triangle>>> tris(n_views);
@@ -104,10 +148,26 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
                         done[i].set_value(std::move(t));
                     }
                 });
-            for (int i = 0; i < n_views && !r; ++i) {
-                const std::vector<hpm_triangle> t = tris[i].get();
-                r = prior_from_triangles(i, dist[i], t.data(), (int)t.size(), sup_w[i], sup_h[i]);
-                if (!r) r = run(i, HPM_MODE_PRIOR, level);
+            if (opt->batch == HPM_RECON_SEQUENTIAL) {
+                for (int i = 0; i < n_views && !r; ++i) {
+                    const std::vector<hpm_triangle> t = tris[i].get();
+                    r = timed(HPM_STAGE_PRIOR, [&]() {
+                        return prior_from_triangles(i, dist[i], t.data(), (int)t.size(), sup_w[i], sup_h[i]);
+                    });
+                    if (!r) r = run(i, HPM_MODE_PRIOR, level);
+                }
+            } else {
+                // a group's priors are built, then its batch runs while later triangulations continue
+                for (int g = 0; g < n_views && !r; g += group) {
+                    const int end = std::min(n_views, g + group);
+                    for (int i = g; i < end && !r; ++i) {
+                        const std::vector<hpm_triangle> t = tris[i].get();
+                        r = timed(HPM_STAGE_PRIOR, [&]() {
+                            return prior_from_triangles(i, dist[i], t.data(), (int)t.size(), sup_w[i], sup_h[i]);
+                        });
+                    }
+                    if (!r) r = run_group(g, end, HPM_MODE_PRIOR, level);
+                }
             }
             for (auto& th : pool) th.join();
             if (r) return r;
@@ -123,10 +183,8 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
                 if (r) return r;
             }
             ++pass;
-            for (int i = 0; i < n_views; ++i) {
-                int r = run(i, mode, level);
-                if (r) return r;
-            }
+            int r = run_pass(mode, level);
+            if (r) return r;
         }
         return HPM_OK;
     };
@@ -159,18 +217,16 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
         if (first) {
             first = false;
             ++pass;
-            for (int i = 0; i < n_views; ++i)
-                if ((rc = run(i, 0, level))) return rc;
+            if ((rc = run_pass(0, level))) return rc;
             if ((rc = prior_passes(level))) return rc;
             if ((rc = geom_passes(level))) return rc;
         } else {
             for (int i = 0; i < n_views; ++i) {
                 int applied = 0;
-                if ((rc = jbu_view(i, &applied))) return rc;
+                if ((rc = timed(HPM_STAGE_JBU, [&]() { return jbu_view(i, &applied); }))) return rc;
             }
             ++pass;
-            for (int i = 0; i < n_views; ++i)
-                if ((rc = run(i, HPM_MODE_HIERARCHY, level))) return rc;
+            if ((rc = run_pass(HPM_MODE_HIERARCHY, level))) return rc;
             if ((rc = prior_passes(level))) return rc;
             if ((rc = geom_passes(level))) return rc;
         }
@@ -190,8 +246,10 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
         }
         if (e != cudaSuccess) return cuda_fail(e, "alloc points");
         int64_t n = 0;
-        rc = consistency_scan(1, n_views, src_off, src_ids, HPM_MAP_DEPTH_GEOM, nullptr, points, (int64_t)total, &n,
-                              nullptr);
+        rc = timed(HPM_STAGE_FUSION, [&]() {
+            return consistency_scan(1, n_views, src_off, src_ids, HPM_MAP_DEPTH_GEOM, nullptr, points, (int64_t)total,
+                                    &n, nullptr);
+        });
         if (rc) return rc;
         n_points = n;
     }

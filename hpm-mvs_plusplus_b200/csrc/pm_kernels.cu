@@ -994,7 +994,8 @@ static cudaError_t sweep_batch_impl(const BatchLaunch& bl, int color, int iter, 
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     if (e != cudaSuccess) return e;
     const int grid = bl.grid_blocks > 0 && bl.grid_blocks < bl.tiles ? bl.grid_blocks : bl.tiles;
-    k<<<grid, dim3(32, BLK / 32), shm, st>>>(bl.args, bl.tile_start, bl.n, color, iter);
+    const int bx = (bl.bx > 0 && bl.bx <= BLK) ? bl.bx : 32;
+    k<<<grid, dim3(bx, BLK / bx), shm, st>>>(bl.args, bl.tile_start, bl.n, color, iter);
     return cudaGetLastError();
 }
 

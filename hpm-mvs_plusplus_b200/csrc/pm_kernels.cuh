@@ -70,6 +70,7 @@ struct BatchLaunch {
     int tiles;        // tile_start[n]
     int max_s;        // largest source count (kernel specialisation)
     int grid_blocks;  // 0 or >= tiles: one block per tile; else a persistent grid of this many blocks
+    int bx;           // half-sweep block width in pixels (32, 16 or 8); the initialisation uses 16 x 8
     bool mand;        // mandatory-consistency kernel
     bool count;       // counting build (hyp_count of every run set)
 };

@@ -144,6 +144,19 @@ int Ctx::fill_run_args(int ref, const int32_t* srcs, int n_src, const hpm_params
 int Ctx::prepare_run(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int texture_level,
                      uint64_t seed, RunArgs& a) {
     cudaSetDevice(device);
+    if (ref < 0 || ref >= HPM_MAX_VIEWS || views[ref].w == 0) return fail(HPM_E_STATE, "reference view %d not set", ref);
+    cudaError_t e = ensure_run((size_t)views[ref].w * views[ref].h);
+    if (e != cudaSuccess) return cuda_fail(e, "alloc run buffers");
+    RunBufs b;
+    b.planes = planes; b.costs = costs; b.pre_costs = pre_costs; b.sel = sel; b.rng = rng; b.conf = conf;
+    return prepare_run_into(ref, srcs, n_src, params, texture_level, seed, b, a);
+}
+
+// The hypothesis reload and run setup of one run (HPM.cpp:741-906, 942-984)
+// into the run buffers `b`: fills `a` and issues the per-run copies and packing
+// kernels on the context's stream.
+int Ctx::prepare_run_into(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int texture_level,
+                          uint64_t seed, const RunBufs& b, RunArgs& a) {
     int rc = fill_run_args(ref, srcs, n_src, params, a);
     if (rc) return rc;
     if (texture_level < 0 || texture_level >= 8) return fail(HPM_E_INVALID, "texture_level must be 0..7");
@@ -155,13 +168,15 @@ int Ctx::prepare_run(int ref, const int32_t* srcs, int n_src, const hpm_params* 
     const bool mand = mode & HPM_MODE_MAND, multi = mode & HPM_MODE_MULTIGEOM;
     if (mand && !geom) return fail(HPM_E_INVALID, "mandatory consistency requires the geometric mode");
     if (!rv.canny || rv.canny_w != W || rv.canny_h != H) return fail(HPM_E_STATE, "view %d has no Canny map of its size", ref);
-    cudaError_t e = ensure_run((size_t)n);
-    if (e != cudaSuccess) return cuda_fail(e, "alloc run buffers");
+    cudaError_t e;
+    float4* const planes = b.planes;
+    float* const costs = b.costs;
+    float* const conf = b.conf;
     a.seed = seed;
-    a.planes = planes; a.costs = costs; a.pre_costs = pre_costs; a.sel = sel; a.rng = rng; a.conf = conf;
+    a.planes = b.planes; a.costs = b.costs; a.pre_costs = b.pre_costs; a.sel = b.sel; a.rng = b.rng; a.conf = b.conf;
     a.canny = rv.canny;
     // selected_views starts at zero at every run (fresh allocation in the reference, HPM.cpp:782)
-    e = cudaMemsetAsync(sel, 0, sizeof(uint32_t) * n, stream);
+    e = cudaMemsetAsync(b.sel, 0, sizeof(uint32_t) * n, stream);
     if (e != cudaSuccess) return cuda_fail(e, "clear view masks");
     const int blocks = (n + 255) / 256;
     const int depth_kind = multi ? HPM_MAP_DEPTH_GEOM : HPM_MAP_DEPTH;
@@ -211,12 +226,16 @@ int Ctx::prepare_run(int ref, const int32_t* srcs, int n_src, const hpm_params* 
         if (!upsample && (nm.w != W || nm.h != H))
             return fail(HPM_E_STATE, "hierarchy: non-upsampled maps must match the image size");
         const int ns = nm.w * nm.h;
-        e = ensure_buf(scaled, scaled_cap, (size_t)ns);
-        if (e != cudaSuccess) return cuda_fail(e, "alloc scaled map");
-        k_pack_scaled<<<(ns + 255) / 256, 256, 0, stream>>>(nm.ptr, upsample ? cm.ptr : dm.ptr, scaled, ns);
+        float4* sc = b.scaled;
+        if (!sc) {
+            e = ensure_buf(scaled, scaled_cap, (size_t)ns);
+            if (e != cudaSuccess) return cuda_fail(e, "alloc scaled map");
+            sc = scaled;
+        }
+        k_pack_scaled<<<(ns + 255) / 256, 256, 0, stream>>>(nm.ptr, upsample ? cm.ptr : dm.ptr, sc, ns);
         k_pack_planes<<<blocks, 256, 0, stream>>>(nullptr, dm.ptr, planes, nullptr, nullptr, n);
         launches += 2;
-        a.scaled = scaled;
+        a.scaled = sc;
         a.prm.scaled_cols = nm.w;
         a.prm.scaled_rows = nm.h;
         if (upsample) a.prm.mode |= HPM_MODE_UPSAMPLE;
@@ -276,8 +295,14 @@ int Ctx::profile_read(hpm_profile* out) {
         float ms = 0.0f;
         e = cudaEventElapsedTime(&ms, prof_events[i].start, prof_events[i].stop);
         if (e != cudaSuccess) return cuda_fail(e, "profiling event time");
-        if (prof_events[i].kind == 0) { out->init_launches++; out->init_ms += ms; }
-        else { out->sweep_launches++; out->sweep_ms += ms; }
+        switch (prof_events[i].kind) {
+        case HPM_STAGE_INIT: out->init_launches++; out->init_ms += ms; break;
+        case HPM_STAGE_SWEEP: out->sweep_launches++; out->sweep_ms += ms; break;
+        case HPM_STAGE_CONFIDENCE: out->confidence_ms += ms; break;
+        case HPM_STAGE_PRIOR: out->prior_ms += ms; break;
+        case HPM_STAGE_JBU: out->jbu_ms += ms; break;
+        default: out->fusion_ms += ms; break;
+        }
     }
     prof_used = 0;
     if (prof_hyp) {
@@ -298,6 +323,12 @@ int Ctx::run_patchmatch(int ref, const int32_t* srcs, int n_src, const hpm_param
     if (rc) return rc;
     rc = launch_schedule(a, 2 * params->max_iterations);
     if (rc) return rc;
+    return finish_run(ref, a, params->mode & HPM_MODE_GEOM);
+}
+
+// GetDepthandNormal (HPM.cu:2829-2842) and the hand-off of the run's results to
+// the view's resident maps (ProcessProblem, main.cpp:599-626).
+int Ctx::finish_run(int ref, const RunArgs& a, bool geom) {
     cudaError_t e;
     if ((e = launch_export(a, stream)) != cudaSuccess) return cuda_fail(e, "export launch");
     ++launches;
@@ -305,16 +336,13 @@ int Ctx::run_patchmatch(int ref, const int32_t* srcs, int n_src, const hpm_param
     const int W = rv.w, H = rv.h;
     const int n = W * H;
     const int blocks = (n + 255) / 256;
-    const bool geom = params->mode & HPM_MODE_GEOM;
-
-    // results -> resident maps (ProcessProblem, main.cpp:599-626)
     const int out_depth = geom ? HPM_MAP_DEPTH_GEOM : HPM_MAP_DEPTH;
     if ((e = ensure_map(ref, out_depth, W, H)) != cudaSuccess) return cuda_fail(e, "alloc depth map");
     if ((e = ensure_map(ref, HPM_MAP_NORMAL, W, H)) != cudaSuccess) return cuda_fail(e, "alloc normal map");
     if ((e = ensure_map(ref, HPM_MAP_COST, W, H)) != cudaSuccess) return cuda_fail(e, "alloc cost map");
-    k_unpack_planes<<<blocks, 256, 0, stream>>>(planes, rv.maps[out_depth].ptr, rv.maps[HPM_MAP_NORMAL].ptr, n);
+    k_unpack_planes<<<blocks, 256, 0, stream>>>(a.planes, rv.maps[out_depth].ptr, rv.maps[HPM_MAP_NORMAL].ptr, n);
     ++launches;
-    e = cudaMemcpyAsync(rv.maps[HPM_MAP_COST].ptr, costs, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream);
+    e = cudaMemcpyAsync(rv.maps[HPM_MAP_COST].ptr, a.costs, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream);
     if (e != cudaSuccess) return cuda_fail(e, "store costs");
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "patchmatch run");

@@ -105,7 +105,8 @@ class _Primitive:
         self.__dict__.update(kw)
 
 
-def _make_primitives(rng: np.random.Generator, textureless_frac: float, n_boxes: int = 1) -> list:
+def _make_primitives(rng: np.random.Generator, textureless_frac: float, n_boxes: int = 1,
+                     box_spread: float = 1.0) -> list:
     prims = []
     tex_size = 512
     # ground plane y = 0 over [-3, 3]^2
@@ -125,7 +126,7 @@ def _make_primitives(rng: np.random.Generator, textureless_frac: float, n_boxes:
                                 tscale=1.0))
     for _ in range(n_boxes):
         half = np.array([rng.uniform(0.15, 0.35), rng.uniform(0.15, 0.4), rng.uniform(0.15, 0.35)])
-        c = np.array([rng.uniform(-1.0, 1.0), half[1], rng.uniform(-1.0, 1.0)])
+        c = np.array([rng.uniform(-box_spread, box_spread), half[1], rng.uniform(-box_spread, box_spread)])
         prims.append(_Primitive("box", c=c, half=half, tscale=1.0))
     for p in prims:
         p.tex = _bandlimited_texture(rng, tex_size, 0.012, 0.06)
@@ -155,7 +156,10 @@ def _sample_tex(tex: torch.Tensor, u: torch.Tensor, v: torch.Tensor) -> torch.Te
     return (t00 * (1 - fx) + t10 * fx) * (1 - fy) + (t01 * (1 - fx) + t11 * fx) * fy
 
 
-def render_view(prims, K, R, t, W, H, noise_rng: np.random.Generator, device, supersample: int = 2):
+def render_view(prims, K, R, t, W, H, noise_rng: np.random.Generator, device, supersample: int = 2,
+                ids_only: bool = False):
+    """Grey image, depth and normals of one view; with ids_only, the index of the primitive seen at each
+    pixel (-1: background) instead."""
     dev = torch.device(device)
     dt = torch.float64
     Kt = torch.tensor(K, dtype=dt, device=dev)
@@ -172,7 +176,8 @@ def render_view(prims, K, R, t, W, H, noise_rng: np.random.Generator, device, su
     best_t = torch.full(px.shape, float("inf"), dtype=dt, device=dev)
     val = torch.zeros(px.shape, dtype=dt, device=dev)
     nrm = torch.zeros(px.shape + (3,), dtype=dt, device=dev)
-    for p in prims:
+    pid = torch.full(px.shape, -1, dtype=torch.int32, device=dev)
+    for pi, p in enumerate(prims):
         tex = torch.tensor(p.tex, dtype=dt, device=dev)
         S = p.tex.shape[0]
         if p.kind == "rect":
@@ -187,9 +192,13 @@ def render_view(prims, K, R, t, W, H, noise_rng: np.random.Generator, device, su
             hit = (tt_ > 1e-6) & (uu.abs() <= p.a) & (vv.abs() <= p.b) & (tt_ < best_t)
             scale = S / (2.0 * p.tscale)
             g = _sample_tex(tex, uu * scale, vv * scale)
+            q = getattr(p, "flat_q", 0.0)
+            if q > 0:  # textureless stripes two scene units apart, a share q of the surface
+                g = torch.where(torch.remainder(uu, 2.0) < 2.0 * q, torch.full_like(g, 0.5), g)
             g = p.lo + (p.hi - p.lo) * g
             best_t = torch.where(hit, tt_, best_t)
             val = torch.where(hit, g, val)
+            pid = torch.where(hit, torch.full_like(pid, pi), pid)
             face_n = nt.expand_as(nrm)
             nrm = torch.where(hit[..., None], face_n, nrm)
         else:  # axis-aligned box, slab test
@@ -215,7 +224,10 @@ def render_view(prims, K, R, t, W, H, noise_rng: np.random.Generator, device, su
             g = p.lo + (p.hi - p.lo) * g
             best_t = torch.where(hit, tn, best_t)
             val = torch.where(hit, g, val)
+            pid = torch.where(hit, torch.full_like(pid, pi), pid)
             nrm = torch.where(hit[..., None], fn, nrm)
+    if ids_only:
+        return pid[ss // 2::ss, ss // 2::ss].cpu().numpy()
     bg = torch.isinf(best_t)
     val = torch.where(bg, torch.full_like(val, 200.0), val)
     # orient normals toward the camera, as PatchMatch hypotheses are
@@ -232,22 +244,77 @@ def render_view(prims, K, R, t, W, H, noise_rng: np.random.Generator, device, su
     return img, depth.cpu().numpy().astype(np.float32), normal.cpu().numpy().astype(np.float32)
 
 
+def _flatten_to_area(prims, cams, target: float, device) -> float:
+    """Makes primitives textureless (std <= 2 grey levels), largest image area first, until they cover about
+    `target` of all views' pixels (measured on 160-pixel-wide renders); returns the covered fraction."""
+    counts = np.zeros(len(prims))
+    total = 0
+    for K, R, t, W, H in cams:
+        s = 160.0 / W
+        Ks = K.copy()
+        Ks[:2] *= s
+        w, h = 160, max(1, int(round(H * s)))
+        ids = render_view(prims, Ks, R, t, w, h, None, device, 1, ids_only=True)
+        total += ids.size
+        for k in range(len(prims)):
+            counts[k] += int((ids == k).sum())
+    frac = counts / max(total, 1)
+    # the ground plane (primitive 0) in flat stripes of the share that reaches the target, then other
+    # surfaces largest first if the whole ground is not enough
+    g = float(frac[0])
+    q = min(1.0, target / g) if g > 0 else 0.0
+    prims[0].flat_q = q
+    covered = g * q
+    for k in [int(k) for k in np.argsort(-frac) if k != 0]:
+        if covered + frac[k] <= target + 0.02 and covered < target - 0.02:
+            prims[k].lo, prims[k].hi = 126.0, 130.0
+            covered += frac[k]
+    return float(covered)
+
+
+def _saturate(img: np.ndarray, frac: float, rng: np.random.Generator) -> np.ndarray:
+    """Specular-like highlights: soft elliptical blobs clipped to 255 over about `frac` of the pixels, placed
+    independently in every view (view-dependent, as specular reflections are)."""
+    H, W = img.shape
+    out = img.astype(np.float32)
+    ys, xs = np.mgrid[0:H, 0:W].astype(np.float32)
+    target = frac * H * W
+    sat = np.zeros((H, W), bool)
+    while sat.sum() < target:
+        cx, cy = rng.uniform(0, W), rng.uniform(0, H)
+        ax, ay = rng.uniform(0.01, 0.04) * W, rng.uniform(0.01, 0.04) * W
+        r2 = ((xs - cx) / ax) ** 2 + ((ys - cy) / ay) ** 2
+        blob = r2 < 1.0
+        out = np.where(r2 < 1.6, np.maximum(out, 255.0 * (1.6 - r2) / 0.6), out)
+        sat |= blob
+    return np.clip(np.rint(out), 0, 255).astype(np.uint8)
+
+
 def make_scene(n_views: int = 5, width: int = 1280, height: int = 960, layout: str = "arc", arc_deg: float = 30.0,
                n_src: int = 4, seed: int = 0, textureless_frac: float = 0.0, device: str = "cpu",
-               sizes: Optional[Sequence[tuple]] = None, supersample: int = 2, n_boxes: int = 1) -> Scene:
-    """Render a seeded scene; `sizes` gives per-view (W, H) for uneven resolutions."""
+               sizes: Optional[Sequence[tuple]] = None, supersample: int = 2, n_boxes: int = 1,
+               textureless_area: float = 0.0, saturated_frac: float = 0.0, box_spread: float = 1.0) -> Scene:
+    """Render a seeded scene; `sizes` gives per-view (W, H) for uneven resolutions.  textureless_area: the
+    share of image area to make textureless (std <= 2 grey levels); saturated_frac: the share of every view
+    covered by saturated specular-like highlights; box_spread: boxes are placed in [-spread, spread]^2."""
     rng = np.random.default_rng(seed)
-    prims = _make_primitives(rng, textureless_frac, n_boxes)
+    prims = _make_primitives(rng, textureless_frac, n_boxes, box_spread)
     centres = _camera_centres(layout, n_views, 4.0, arc_deg)
     target = np.array([0.0, 0.3, 0.0])
-    views = []
+    cams = []
     for i, C in enumerate(centres):
         W, H = (sizes[i] if sizes is not None else (width, height))
         R, t = _look_at(C, target)
         f = 0.9 * W
         K = np.array([[f, 0.0, (W - 1) / 2.0], [0.0, f, (H - 1) / 2.0], [0.0, 0.0, 1.0]])
+        cams.append((K, R, t, W, H))
+    flat_area = _flatten_to_area(prims, cams, textureless_area, device) if textureless_area > 0 else 0.0
+    views = []
+    for i, (K, R, t, W, H) in enumerate(cams):
         noise_rng = np.random.default_rng(seed * 1000003 + i)
         gray, depth, normal = render_view(prims, K, R, t, W, H, noise_rng, device, supersample)
+        if saturated_frac > 0:
+            gray = _saturate(gray, saturated_frac, np.random.default_rng(seed * 7919 + i))
         img = np.repeat(gray[..., None], 3, axis=2)
         valid = depth[depth > 0]
         views.append(SceneView(img, K.astype(np.float32), R.astype(np.float32), t.astype(np.float32), depth, normal,
@@ -270,7 +337,42 @@ def make_scene(n_views: int = 5, width: int = 1280, height: int = 960, layout: s
             cand.append((j, 100.0 / (1.0 + ang)))
         cand.sort(key=lambda x: -x[1])
         pairs.append(cand[:n_src])
-    return Scene(views, pairs, seed, {"layout": layout, "n_views": n_views, "textureless_frac": textureless_frac})
+    return Scene(views, pairs, seed, {"layout": layout, "n_views": n_views, "textureless_frac": textureless_frac,
+                                      "textureless_area": flat_area, "saturated_frac": saturated_frac})
+
+
+# The five workloads of the benchmark, at their full sizes (seeded).
+CONFIGS = {
+    "c1": "5 views 1280x960 on a 30-degree arc, 4 sources, --initial-image-scale 4",
+    "c2": "49 views 1600x1200 on a two-ring hemisphere, 10 sources, --initial-image-scale 1",
+    "c3": "49 views 1600x1200 hemisphere, 10 sources, about 40 % of the image area textureless (std <= 2)",
+    "c4": "20 views 1024x768 on a two-ring hemisphere, 10 sources, --initial-image-scale 1",
+    "c5": "120 views of uneven sizes (40 x 3072x2048, 40 x 1920x1080, 40 x 1024x768), ground plane and 30 boxes, "
+          "5 % saturated specular-like patches, 10 sources",
+}
+
+
+def make_config(name: str, seed: int = 2024, device: str = "cpu", n_views: Optional[int] = None) -> Scene:
+    """The scene of workload `name` (c1..c5); n_views overrides the view count (c5 keeps its size mix)."""
+    if name == "c1":
+        return make_scene(n_views=n_views or 5, width=1280, height=960, layout="arc", n_src=4, seed=seed,
+                          device=device)
+    if name == "c2":
+        return make_scene(n_views=n_views or 49, width=1600, height=1200, layout="hemisphere", n_src=10, seed=seed,
+                          device=device)
+    if name == "c3":
+        return make_scene(n_views=n_views or 49, width=1600, height=1200, layout="hemisphere", n_src=10, seed=seed,
+                          device=device, textureless_area=0.4)
+    if name == "c4":
+        return make_scene(n_views=n_views or 20, width=1024, height=768, layout="hemisphere", n_src=10, seed=seed,
+                          device=device)
+    if name == "c5":
+        n = n_views or 120
+        mix = [(3072, 2048), (1920, 1080), (1024, 768)]
+        sizes = [mix[i % 3] for i in range(n)]
+        return make_scene(n_views=n, layout="mixed", n_src=min(10, n - 1), seed=seed, device=device, sizes=sizes,
+                          n_boxes=30, box_spread=2.5, saturated_frac=0.05)
+    raise ValueError(f"unknown workload {name!r} (c1..c5)")
 
 
 def write_dense_folder(scene: Scene, folder: str) -> None:

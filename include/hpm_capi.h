@@ -35,8 +35,16 @@ typedef struct hpm_recon_options {
     int32_t fuse;                /* run fusion after the last level */
     int32_t level_max_side;      /* 0: 1000, the pyramid bound of ComputeMultiScaleSettings (main.cpp:205);
                                     smaller values build more levels on small inputs */
+    int32_t batch;               /* batching form (hpm_run_batch): HPM_RECON_SEQUENTIAL runs the views of a
+                                    pass one after another as main.cpp:1253-1255 does; HPM_RECON_BATCH_EXACT
+                                    batches every pass whose runs read no map of the same pass (same
+                                    result); HPM_RECON_BATCH_ALL also batches the multi-geometry passes,
+                                    which then read the previous pass's depth maps (Jacobi) */
+    int32_t batch_views;         /* views per batch (0: all views of the pass) */
     uint64_t seed;               /* key of the random streams of all runs */
 } hpm_recon_options;
+
+enum { HPM_RECON_SEQUENTIAL = 0, HPM_RECON_BATCH_EXACT = 1, HPM_RECON_BATCH_ALL = 2 };
 
 enum {
     HPM_OK = 0,
@@ -98,6 +106,34 @@ int hpm_set_prior(hpm_ctx *ctx, int view, const float *planes, const uint8_t *ma
  * keys the counter-based random stream of this run. */
 int hpm_run_patchmatch(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, const hpm_params *params,
                        int texture_level, uint64_t seed);
+
+/* Batching form: n PatchMatch runs -- reference view refs[k] against sources
+ * src_ids[src_off[k] .. src_off[k+1]) with params[k] and seeds[k] -- in one
+ * launch per stage (initialisation, each half-sweep) over all n views.  It
+ * replaces the per-view loop of main.cpp:1253-1255 around HPM::RunPatchMatch
+ * (HPM.cu:2987-3035), which launches and synchronises one view at a time.
+ * Inputs and outputs are those of hpm_run_patchmatch for each run.  Every run
+ * reads the resident maps as they were before the call and writes its outputs
+ * after all runs have finished, so the result equals n calls of
+ * hpm_run_patchmatch in order whenever no run reads a map another run of the
+ * batch writes (the photometric, prior, hierarchy and first geometric passes);
+ * in multi-geometry passes it is the Jacobi form of the reference's
+ * Gauss-Seidel view loop.  All runs share one mode and iteration count; a view
+ * appears at most once.  Run buffers for all n views stay resident. */
+int hpm_run_batch(hpm_ctx *ctx, int n, const int32_t *refs, const int32_t *src_off, const int32_t *src_ids,
+                  const hpm_params *params, int texture_level, const uint64_t *seeds);
+
+/* Options of hpm_run_batch (bit set; default HPM_BATCH_AUTOTUNE):
+ *   HPM_BATCH_AUTOTUNE    the first batch of each (source count, mode, size class)
+ *                         times the candidate launch shapes of the half-sweep (block
+ *                         width 32, 16 or 8 pixels; one block per tile or a persistent
+ *                         grid) on a copy of its state and keeps the fastest; results
+ *                         do not depend on the shape
+ *   HPM_BATCH_GRAPH       the initialisation and half-sweeps of a batch are captured once
+ *                         per batch shape in a CUDA graph and replayed */
+#define HPM_BATCH_AUTOTUNE 1
+#define HPM_BATCH_GRAPH 2
+int hpm_set_batch_options(hpm_ctx *ctx, int flags);
 
 /* Fixed-hypothesis costs (no reference counterpart: parity entry point).
  * out[k*n_src + j] = bilateral NCC (HPM.cu:375-448) of pixel (px[2k], px[2k+1])
@@ -272,6 +308,10 @@ typedef struct hpm_profile {
     double sweep_ms;
     uint64_t init_view_evals;  /* (hypothesis, source view) pairs costed, each 36 patch samples, */
     uint64_t sweep_view_evals; /*   every hypothesis against all S sources as the reference does */
+    double confidence_ms;      /* device time of hpm_reconstruct's other stages: ConfidenceEvaluation, */
+    double prior_ms;           /*   prior construction (support points, raster, fits, reload; the host */
+    double jbu_ms;             /*   Delaunay triangulations overlap it and are not included), JBU and */
+    double fusion_ms;          /*   fusion */
 } hpm_profile;
 
 /* Turns profiling on (flags) or off (0).  Timing adds two event records per
