@@ -44,8 +44,11 @@ EXPORTED_SYMBOLS = (
     "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior", "hpm_set_image", "hpm_prepare_level",
     "hpm_get_level", "hpm_reconstruct", "hpm_get_points", "hpm_get_stream", "hpm_profile_enable",
     "hpm_profile_read", "hpm_measure_fp32_peak", "hpm_eval_costs_noalloc", "hpm_eval_cost_grad", "hpm_gn_refine",
-    "hpm_set_texture_format", "hpm_run_batch", "hpm_set_batch_options",
+    "hpm_set_texture_format", "hpm_run_batch", "hpm_set_batch_options", "hpm_set_ncc_mode",
 )
+
+NCC_PLAIN = 0
+NCC_SHIFTED = 1
 
 BATCH_AUTOTUNE = 1
 BATCH_GRAPH = 2
@@ -200,6 +203,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                    vp]
     lib.hpm_run_batch.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, ctypes.c_int, vp]
     lib.hpm_set_batch_options.argtypes = [vp, ctypes.c_int]
+    lib.hpm_set_ncc_mode.argtypes = [vp, ctypes.c_int]
     lib.hpm_eval_costs_noalloc.argtypes = lib.hpm_eval_costs.argtypes
     lib.hpm_eval_cost_grad.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int, vp,
                                        vp, vp, vp]
@@ -296,6 +300,10 @@ class Context:
     def set_texture_format(self, fmt: int) -> None:
         """TEX_F32 or TEX_F16 texels for the source images bound from now on (hpm_set_texture_format)."""
         self._check(self.lib.hpm_set_texture_format(self.h, fmt), "hpm_set_texture_format")
+
+    def set_ncc_mode(self, mode: int) -> None:
+        """NCC_PLAIN or NCC_SHIFTED (shifted moments, the precision form) from now on (hpm_set_ncc_mode)."""
+        self._check(self.lib.hpm_set_ncc_mode(self.h, mode), "hpm_set_ncc_mode")
 
     def set_address_mode(self, mode: int) -> None:
         self._check(self.lib.hpm_set_address_mode(self.h, mode), "hpm_set_address_mode")

@@ -190,6 +190,15 @@ int hpm_set_texture_format(hpm_ctx* ctx, int format) {
     return HPM_OK;
 }
 
+int hpm_set_ncc_mode(hpm_ctx* ctx, int mode) {
+    if (!ctx) return HPM_E_INVALID;
+    Ctx* c = reinterpret_cast<Ctx*>(ctx);
+    if (mode != HPM_NCC_PLAIN && mode != HPM_NCC_SHIFTED)
+        return c->fail(HPM_E_INVALID, "NCC mode must be HPM_NCC_PLAIN or HPM_NCC_SHIFTED");
+    c->ncc_mode = mode;
+    return HPM_OK;
+}
+
 int64_t hpm_launch_count(const hpm_ctx* ctx) { return ctx ? reinterpret_cast<const Ctx*>(ctx)->launches : 0; }
 
 int hpm_synchronize(hpm_ctx* ctx) {

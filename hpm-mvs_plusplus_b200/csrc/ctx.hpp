@@ -78,7 +78,8 @@ struct Ctx {
     std::string err;
     std::vector<ViewState> views;
     int addr_mode = 0;
-    int tex_format = 0;  // HPM_TEX_F32 or HPM_TEX_F16: texel type of the source-image textures
+    int tex_format = 0;  // HPM_TEX_F32, HPM_TEX_F16 or HPM_TEX_U8: texel type of the source-image textures
+    int ncc_mode = 0;    // HPM_NCC_PLAIN or HPM_NCC_SHIFTED
     uint16_t* half_stage = nullptr; size_t half_stage_cap = 0;
     int64_t launches = 0;
 

@@ -59,6 +59,8 @@ __device__ __forceinline__ void build_patch(const RunArgs& a, int px, int py, Pa
     const float center = __ldg(ref + (size_t)clampi(py, 0, H - 1) * W + clampi(px, 0, W - 1));
     const float two_ss = 2.0f * a.prm.sigma_spatial * a.prm.sigma_spatial;
     const float two_sc = 2.0f * a.prm.sigma_color * a.prm.sigma_color;
+    // shifted moments (precision form): the patch relative to its centre texel; shift 0 is the plain arithmetic
+    const float cs = a.ncc_shift ? center : 0.0f;
     float s_r = 0.f, s_rr = 0.f, s_w = 0.f;
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
@@ -71,10 +73,11 @@ __device__ __forceinline__ void build_patch(const RunArgs& a, int px, int py, Pa
             const float r = __ldg(ref + (size_t)clampi(py + dy, 0, H - 1) * W + x);
             const float sd = sqrtf((float)(dx * dx + dy * dy));
             const float w = hpm_expf(-sd / two_ss - fabsf(r - center) / two_sc);
-            const float wr = w * r;
+            const float rs = r - cs;
+            const float wr = w * rs;
             P.p[i * 6 + j] = make_float2(w, wr);
             r_r += wr;
-            r_rr = hpm_fma(wr, r, r_rr);
+            r_rr = hpm_fma(wr, rs, r_rr);
             r_w += w;
         }
         s_r += r_r; s_rr += r_rr; s_w += r_w;
@@ -116,6 +119,7 @@ __device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int 
     }
     const cudaTextureObject_t tex = a.tex[j + 1];
     float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
+    float vshift = 0.0f;  // shifted moments: the source patch relative to its first sample
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         const float x = (float)(px - kPatchRadius + kPatchStep * i);
@@ -129,14 +133,16 @@ __device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int 
             const float iz = hpm_recip_near(qz, iz_c);
             v[k] = tex2D<float>(tex, hpm_fma(qx, iz, 0.5f), hpm_fma(qy, iz, 0.5f));
         }
+        if (i == 0 && a.ncc_shift) vshift = v[0];
         float r_s = 0.f, r_ss = 0.f, r_rs = 0.f;
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             const float2 w = P.p[i * 6 + k];
-            const float ws = w.x * v[k];
+            const float vk = v[k] - vshift;
+            const float ws = w.x * vk;
             r_s += ws;
-            r_ss = hpm_fma(ws, v[k], r_ss);
-            r_rs = hpm_fma(w.y, v[k], r_rs);
+            r_ss = hpm_fma(ws, vk, r_ss);
+            r_rs = hpm_fma(w.y, vk, r_rs);
         }
         s_s += r_s; s_ss += r_ss; s_rs += r_rs;
     }

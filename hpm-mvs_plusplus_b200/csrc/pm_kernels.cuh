@@ -23,6 +23,7 @@ struct RunArgs {
     ViewBasis fwd[32], bwd[32];     // geometric cost: point transfer reference -> source j+1 and back            // homography basis of source j+1 w.r.t. the reference
     float kinv[4];                  // 1/fx, 1/fy, cx/fx, cy/fy of the reference camera
     float var_s_min;                // flat-source threshold: 1e-5 (HPM.cu:434) in the textures' grey units
+    int ncc_shift;                  // 1: shifted NCC moments (precision form); 0: the plain arithmetic
     cudaTextureObject_t tex[32];    // linear-filtered source images (index j+1)
     const float* depth_src[32];     // geometric mode: source depth maps (index j+1)
     int dsw[32], dsh[32];           // their sizes

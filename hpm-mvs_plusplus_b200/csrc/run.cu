@@ -130,6 +130,7 @@ int Ctx::fill_run_args(int ref, const int32_t* srcs, int n_src, const hpm_params
     hpm_ref_kinv(&rv.cam, a.kinv);
     // 8-bit textures return grey / 255; the NCC is scale-free, only the flat-source test scales
     a.var_s_min = tex_format == HPM_TEX_U8 ? 1e-5f / (255.0f * 255.0f) : 1e-5f;
+    a.ncc_shift = ncc_mode == HPM_NCC_SHIFTED ? 1 : 0;
     a.ref_img = rv.gray;
     a.prm = *params;
     a.S = n_src;

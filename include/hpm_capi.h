@@ -285,6 +285,17 @@ int hpm_set_address_mode(hpm_ctx *ctx, int mode);
 #define HPM_TEX_U8 2  /* 8-bit texels read as grey/255; the NCC is scale-free, its flat-source test is rescaled */
 int hpm_set_texture_format(hpm_ctx *ctx, int format);
 
+/* Arithmetic of the bilateral NCC moments (HPM.cu:375-448) from now on:
+ * HPM_NCC_PLAIN (default) forms the variances as E[x^2] - E[x]^2 as the
+ * reference does; HPM_NCC_SHIFTED, the precision form, accumulates the
+ * reference patch relative to its centre texel and each source patch relative
+ * to its first sample, so that flat (textureless) patches keep their variance
+ * instead of losing it to cancellation.  The NCC is shift-invariant: the two
+ * differ only by rounding, which the shifted form makes smaller. */
+#define HPM_NCC_PLAIN 0
+#define HPM_NCC_SHIFTED 1
+int hpm_set_ncc_mode(hpm_ctx *ctx, int mode);
+
 /* Kernel launches issued by this context since creation (for accounting). */
 int64_t hpm_launch_count(const hpm_ctx *ctx);
 

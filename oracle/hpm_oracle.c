@@ -32,6 +32,14 @@ static int g_tex_model = 0;
 void ora_set_texture_model(int model) { g_tex_model = model; }
 int ora_get_texture_model(void) { return g_tex_model; }
 
+/* Shifted moments in the NCC (the precision form): the reference patch is
+ * accumulated relative to its centre texel and the source patch relative to
+ * its first sample, so flat patches keep their variance instead of losing it
+ * to E[x^2] - E[x]^2 cancellation.  Off (shift 0) gives the plain arithmetic
+ * bit for bit. */
+static int g_ncc_shift = 0;
+void ora_set_ncc_shift(int on) { g_ncc_shift = on != 0; }
+
 /* float -> int conversion with the semantics of the GPU's cvt.rzi.s32.f32:
  * truncation toward zero, NaN -> 0, saturation at the int range. */
 static inline int f2i_rz(float v)
@@ -251,6 +259,7 @@ float ora_bilateral_ncc(const float *ref, const hpm_camera *rc, const float *src
     const float center = texel(ref, rw, rh, px, py);
     const float two_ss = 2.0f * prm->sigma_spatial * prm->sigma_spatial;
     const float two_sc = 2.0f * prm->sigma_color * prm->sigma_color;
+    const float cs = g_ncc_shift ? center : 0.0f;
     float pw[36], pwr[36];
     float s_r = 0.f, s_rr = 0.f, s_w = 0.f;
     for (int i = 0; i < 6; ++i) {
@@ -261,11 +270,12 @@ float ora_bilateral_ncc(const float *ref, const hpm_camera *rc, const float *src
             const float r = texel(ref, rw, rh, px + dx, py + dy);
             const float sd = sqrtf((float)(dx * dx + dy * dy));
             const float w = hpm_expf(-sd / two_ss - fabsf(r - center) / two_sc);
-            const float wr = w * r;
+            const float rs = r - cs;
+            const float wr = w * rs;
             pw[i * 6 + j] = w;
             pwr[i * 6 + j] = wr;
             r_r += wr;
-            r_rr = hpm_fma(wr, r, r_rr);
+            r_rr = hpm_fma(wr, rs, r_rr);
             r_w += w;
         }
         s_r += r_r; s_rr += r_rr; s_w += r_w;
@@ -293,6 +303,7 @@ float ora_bilateral_ncc(const float *ref, const hpm_camera *rc, const float *src
         if (ux >= sw || ux < 0.0f || uy >= sh || uy < 0.0f) return cost_max;
     }
     float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
+    float vshift = 0.0f;
     for (int i = 0; i < 6; ++i) {
         const float x = (float)(px - 5 + 2 * i);
         float r_s = 0.f, r_ss = 0.f, r_rs = 0.f;
@@ -302,7 +313,9 @@ float ora_bilateral_ncc(const float *ref, const hpm_camera *rc, const float *src
             const float qy = hpm_fma(H[3], x, hpm_fma(H[4], y, H[5]));
             const float qz = hpm_fma(H[6], x, hpm_fma(H[7], y, H[8]));
             const float iz = hpm_recip_near(qz, iz_c);
-            const float v = ora_tex2d(src, sw, sh, hpm_fma(qx, iz, 0.5f), hpm_fma(qy, iz, 0.5f));
+            const float v0 = ora_tex2d(src, sw, sh, hpm_fma(qx, iz, 0.5f), hpm_fma(qy, iz, 0.5f));
+            if (g_ncc_shift && i == 0 && k == 0) vshift = v0;
+            const float v = v0 - vshift;
             const float ws = pw[i * 6 + k] * v;
             r_s += ws;
             r_ss = hpm_fma(ws, v, r_ss);
@@ -319,6 +332,91 @@ float ora_bilateral_ncc(const float *ref, const hpm_camera *rc, const float *src
     /* max(0, min(2, c)) with fminf/fmaxf NaN semantics (the non-NaN operand wins) */
     c = fminf(cost_max, c);
     c = fmaxf(0.0f, c);
+    return c;
+}
+
+double ora_bilateral_ncc64(const float *ref, const hpm_camera *rc, const float *src, const hpm_camera *sc,
+                        int px, int py, const float plane[4], const hpm_params *prm)
+{
+    /* ora_bilateral_ncc with the same weights and the same float sample
+     * positions and filtered samples, but every moment accumulated and the
+     * NCC formed in double: the reference the precision form's accumulation
+     * errors are measured against. */
+    const float cost_max = 2.0f;
+    const int rw = rc->width, rh = rc->height, sw = sc->width, sh = sc->height;
+    const float center = texel(ref, rw, rh, px, py);
+    const float two_ss = 2.0f * prm->sigma_spatial * prm->sigma_spatial;
+    const float two_sc = 2.0f * prm->sigma_color * prm->sigma_color;
+    double pw[36];
+    double s_r = 0, s_w = 0;
+    for (int i = 0; i < 6; ++i) {
+        const int dx = -5 + 2 * i;
+        for (int j = 0; j < 6; ++j) {
+            const int dy = -5 + 2 * j;
+            const float r = texel(ref, rw, rh, px + dx, py + dy);
+            const float sd = sqrtf((float)(dx * dx + dy * dy));
+            const float w = hpm_expf(-sd / two_ss - fabsf(r - center) / two_sc);
+            pw[i * 6 + j] = w;
+            s_r += (double)w * r;
+            s_w += w;
+        }
+    }
+    const double mean_r = s_r / s_w;
+    double var_r = 0;
+    for (int i = 0; i < 36; ++i) {
+        const int dx = -5 + 2 * (i / 6), dy = -5 + 2 * (i % 6);
+        const double d = (double)texel(ref, rw, rh, px + dx, py + dy) - mean_r;
+        var_r += pw[i] * d * d;
+    }
+    var_r /= s_w;
+    const float kMinVar = 1e-5f;
+    if (var_r < kMinVar) return cost_max;
+
+    /* homography factored as H = A - b m^T (include/hpm_geometry.h) */
+    float A[9], bv[3], kinv[4], m[3], H[9];
+    hpm_view_basis(rc, sc, A, bv);
+    hpm_ref_kinv(rc, kinv);
+    hpm_plane_m(kinv, plane[0], plane[1], plane[2], plane[3], m);
+    hpm_homography(A, bv, m, H);
+    float iz_c;
+    {
+        const float fx = (float)px, fy = (float)py;
+        const float cx = hpm_fma(H[0], fx, hpm_fma(H[1], fy, H[2]));
+        const float cy = hpm_fma(H[3], fx, hpm_fma(H[4], fy, H[5]));
+        const float cz = hpm_fma(H[6], fx, hpm_fma(H[7], fy, H[8]));
+        iz_c = 1.0f / cz;
+        const float ux = cx * iz_c, uy = cy * iz_c;
+        if (ux >= sw || ux < 0.0f || uy >= sh || uy < 0.0f) return cost_max;
+    }
+    double vals[36];
+    for (int i = 0; i < 6; ++i) {
+        const float x = (float)(px - 5 + 2 * i);
+        for (int k = 0; k < 6; ++k) {
+            const float y = (float)(py - 5 + 2 * k);
+            const float qx = hpm_fma(H[0], x, hpm_fma(H[1], y, H[2]));
+            const float qy = hpm_fma(H[3], x, hpm_fma(H[4], y, H[5]));
+            const float qz = hpm_fma(H[6], x, hpm_fma(H[7], y, H[8]));
+            const float iz = hpm_recip_near(qz, iz_c);
+            vals[i * 6 + k] = ora_tex2d(src, sw, sh, hpm_fma(qx, iz, 0.5f), hpm_fma(qy, iz, 0.5f));
+        }
+    }
+    /* two-pass moments in double */
+    double mean_s = 0;
+    for (int i = 0; i < 36; ++i) mean_s += pw[i] * vals[i];
+    mean_s /= s_w;
+    double var_s = 0, cov = 0;
+    for (int i = 0; i < 36; ++i) {
+        const int dx = -5 + 2 * (i / 6), dy = -5 + 2 * (i % 6);
+        const double dr = (double)texel(ref, rw, rh, px + dx, py + dy) - mean_r;
+        const double ds = vals[i] - mean_s;
+        var_s += pw[i] * ds * ds;
+        cov += pw[i] * dr * ds;
+    }
+    var_s /= s_w;
+    cov /= s_w;
+    if (var_s < kMinVar) return cost_max;
+    double c = 1.0 - cov / sqrt(var_r * var_s);
+    c = c < 0.0 ? 0.0 : (c > 2.0 ? 2.0 : c);
     return c;
 }
 

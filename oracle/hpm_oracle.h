@@ -61,6 +61,11 @@ typedef struct ora_state {
 /* Texture filter model: 0 = as measured on B200 (8-bit weights and 8-bit cross
  * weight), 1 = separable 8-bit weights of the CUDA Programming Guide. */
 void ora_set_texture_model(int model);
+/* Shifted-moment NCC of the precision form (0: plain arithmetic). */
+void ora_set_ncc_shift(int on);
+/* The bilateral NCC of ora_bilateral_ncc's own samples with its moments in double. */
+double ora_bilateral_ncc64(const float *ref, const hpm_camera *ref_cam, const float *src, const hpm_camera *src_cam,
+                           int px, int py, const float plane[4], const hpm_params *prm);
 int ora_get_texture_model(void);
 float ora_tex2d(const float *img, int width, int height, float x, float y);
 

@@ -79,6 +79,9 @@ def lib() -> ctypes.CDLL:
         L.ora_texture.restype = ctypes.c_float
         L.ora_texture.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.ora_set_texture_model.argtypes = [ctypes.c_int]
+        L.ora_set_ncc_shift.argtypes = [ctypes.c_int]
+        L.ora_bilateral_ncc64.restype = ctypes.c_double
+        L.ora_bilateral_ncc64.argtypes = L.ora_bilateral_ncc.argtypes
         for fn in ("ora_random_init",):
             getattr(L, fn).argtypes = [vp, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.POINTER(State),
                                        ctypes.c_uint64, ctypes.c_uint32]
@@ -146,6 +149,22 @@ def uniform(seed: int, view: int, x: int, y: int, draw: int) -> float:
 
 def set_texture_model(model: int) -> None:
     lib().ora_set_texture_model(model)
+
+
+def set_ncc_shift(on: bool) -> None:
+    """Shifted-moment NCC of the precision form in every oracle cost (off: the plain arithmetic)."""
+    lib().ora_set_ncc_shift(1 if on else 0)
+
+
+def ncc64(ref, ref_cam, src, src_cam, params, px: int, py: int, plane) -> float:
+    """The bilateral NCC of the oracle's own samples (same positions and filter model) with double moments."""
+    r = np.ascontiguousarray(ref, np.float32)
+    s = np.ascontiguousarray(src, np.float32)
+    pl = np.ascontiguousarray(plane, np.float32)
+    rc, sc = to_cam(ref_cam), to_cam(src_cam)
+    prm = to_params(params)
+    return lib().ora_bilateral_ncc64(_p(r), ctypes.byref(rc), _p(s), ctypes.byref(sc), px, py, _p(pl),
+                                     ctypes.byref(prm))
 
 
 def tex2d(img: np.ndarray, x: float, y: float) -> float:
