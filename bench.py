@@ -334,6 +334,10 @@ def run_ours(args, scene, rank, world, local_rank):
     launches_per_step = prof.sweep_launches / max(args.steps, 1)
     achieved = flops_per_step / (sweep_ms_per_step * 1e-3) / 1e12 if sweep_ms_per_step > 0 else None
     traffic = _ncu_traffic()
+    # the unit that binds the half-sweep: the texture unit's linear filtering, one fetch per patch sample
+    tex_peak = hb.measure_tex_peak(local_rank, hb.TEX_F32)
+    sampled_per_step = counted.sweep_sampled * SAMPLES_PER_NCC
+    tex_achieved = sampled_per_step / (sweep_ms_per_step * 1e-3) / 1e9 if sweep_ms_per_step > 0 else None
     roofline = {
         "kernel": "k_half_sweep", "bound": "fp32", "unit": "TFLOP/s",
         "achieved": achieved, "peak": fp32_peak,
@@ -346,6 +350,17 @@ def run_ours(args, scene, rank, world, local_rank):
         "share_of_step": (sweep_ms_per_step / (dev_ms / args.steps / world)) if dev_ms > 0 else None,
         "cost_evals_per_s": evals_per_step / (sweep_ms_per_step * 1e-3) if sweep_ms_per_step > 0 else None,
         "hbm_peak_gbs": _measured_hbm(),
+        "texture": {"unit": "Gfetch/s", "achieved": tex_achieved, "peak": tex_peak,
+                    "frac": (tex_achieved / tex_peak) if tex_achieved and tex_peak else None,
+                    "peak_source": "hpm_measure_tex_peak: linear-filtered F32 fetches in the half-sweep's access "
+                                   "pattern on this GPU",
+                    "fetches_per_step": sampled_per_step,
+                    "note": "executed work: NCCs that sampled the source (zero-weight views, out-of-image centres "
+                            "and flat reference patches skip sampling), 36 fetches each"},
+        "fp32_executed": {"achieved": (sampled_per_step * ALGO_FLOPS_PER_EVAL / (sweep_ms_per_step * 1e-3) / 1e12)
+                          if sweep_ms_per_step > 0 else None,
+                          "frac": (sampled_per_step * ALGO_FLOPS_PER_EVAL / (sweep_ms_per_step * 1e-3) / 1e12
+                                   / fp32_peak) if sweep_ms_per_step > 0 and fp32_peak else None},
     }
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

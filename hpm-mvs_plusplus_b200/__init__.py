@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = (
     "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior", "hpm_set_image", "hpm_prepare_level",
     "hpm_get_level", "hpm_reconstruct", "hpm_get_points", "hpm_get_stream", "hpm_profile_enable",
     "hpm_profile_read", "hpm_measure_fp32_peak", "hpm_eval_costs_noalloc", "hpm_eval_cost_grad", "hpm_gn_refine",
-    "hpm_set_texture_format", "hpm_run_batch", "hpm_set_batch_options", "hpm_set_ncc_mode",
+    "hpm_set_texture_format", "hpm_run_batch", "hpm_set_batch_options", "hpm_set_ncc_mode", "hpm_measure_tex_peak",
 )
 
 NCC_PLAIN = 0
@@ -71,6 +71,7 @@ class Profile(ctypes.Structure):
     _fields_ = [("init_launches", ctypes.c_int64), ("sweep_launches", ctypes.c_int64),
                 ("init_ms", ctypes.c_double), ("sweep_ms", ctypes.c_double),
                 ("init_view_evals", ctypes.c_uint64), ("sweep_view_evals", ctypes.c_uint64),
+                ("sweep_sampled", ctypes.c_uint64),
                 ("confidence_ms", ctypes.c_double), ("prior_ms", ctypes.c_double), ("jbu_ms", ctypes.c_double),
                 ("fusion_ms", ctypes.c_double)]
 
@@ -239,6 +240,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.hpm_profile_enable.argtypes = [vp, ctypes.c_int]
     lib.hpm_profile_read.argtypes = [vp, ctypes.POINTER(Profile)]
     lib.hpm_measure_fp32_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.hpm_measure_tex_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTED_SYMBOLS:
         getattr(lib, name)
     del i32, f
@@ -586,3 +588,13 @@ class View:
 
     gray: np.ndarray  # float32 H x W
     cam: Camera
+
+
+def measure_tex_peak(device: int = 0, fmt: int = TEX_F32) -> float:
+    """Linear-filtered texture fetches per second of the device, in 1e9/s (hpm_measure_tex_peak)."""
+    lib = load_library()
+    out = ctypes.c_double()
+    rc = lib.hpm_measure_tex_peak(device, fmt, ctypes.byref(out))
+    if rc != 0:
+        raise HPMError(f"hpm_measure_tex_peak failed ({rc})")
+    return out.value

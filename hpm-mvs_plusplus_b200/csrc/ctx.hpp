@@ -133,7 +133,7 @@ struct Ctx {
     struct TimedLaunch { cudaEvent_t start, stop; int kind; };
     std::vector<TimedLaunch> prof_events;  // pool; the first prof_used are pending
     size_t prof_used = 0;
-    unsigned long long* prof_hyp = nullptr;  // device counters [init, sweep]
+    unsigned long long* prof_hyp = nullptr;  // device counters [init, sweep credited, sweep sampled]
     int record_start(int kind, TimedLaunch*& slot);
     int profile_read(hpm_profile* out);
 

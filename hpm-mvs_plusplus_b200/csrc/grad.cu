@@ -28,9 +28,18 @@ struct SrcImages {
 
 namespace {
 
+// Self-check of the gradient kernels: an index outside its buffer (which the
+// clamping below rules out) is counted here and the access skipped, so a
+// wrong index surfaces as an error status instead of a memory fault.
+__device__ unsigned int g_grad_oob;
+
 __device__ __forceinline__ float texel_c(const float* img, int w, int h, int x, int y) {
     x = min(max(x, 0), w - 1);
     y = min(max(y, 0), h - 1);
+    if (!img || x < 0 || y < 0 || w <= 0 || h <= 0) {
+        atomicAdd(&g_grad_oob, 1u);
+        return 0.0f;
+    }
     return __ldg(img + (size_t)y * w + x);
 }
 
@@ -96,6 +105,10 @@ __device__ float cost_grad_view(const RunArgs& a, const SrcImages& si, const Ref
     for (int r = 0; r < 3; ++r)
 #pragma unroll
         for (int k = 0; k < 3; ++k) H[3 * r + k] = A[3 * r + k] - b[r] * m[k];
+    if (j < 0 || j > 30) {
+        atomicAdd(&g_grad_oob, 1u);
+        return 2.0f;
+    }
     const float* img = si.img[j + 1];
     const int sw = si.w[j + 1], sh = si.h[j + 1];
     {
@@ -154,6 +167,10 @@ __global__ void k_cost_grad(const __grid_constant__ RunArgs a, const __grid_cons
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int x = px[2 * k], y = px[2 * k + 1];
+    if (x < 0 || x >= a.W || y < 0 || y >= a.H) {
+        atomicAdd(&g_grad_oob, 1u);
+        return;
+    }
     RefPatch P;
     ref_patch(a, x, y, P);
     const float th[3] = { theta[3 * k], theta[3 * k + 1], theta[3 * k + 2] };
@@ -184,11 +201,16 @@ __device__ bool solve3(const float M[9], const float rhs[3], float d[3]) {
 // grows tenfold on every rejected step; the valid views are those with a cost
 // in (0, 2) at the start.  Depth stays in [dmin, dmax].
 __global__ void k_gn_refine(const __grid_constant__ RunArgs a, const __grid_constant__ SrcImages si, int steps,
-                            float* __restrict__ depth, float* __restrict__ normal, float* __restrict__ cost_out) {
+                            float* __restrict__ depth, float* __restrict__ normal, float* __restrict__ cost_out,
+                            size_t n_px) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.W || y >= a.H) return;
     const size_t i = (size_t)y * a.W + x;
+    if (i >= n_px) {
+        atomicAdd(&g_grad_oob, 1u);
+        return;
+    }
     const hpm_camera& c0 = a.cams[0];
     float d0 = depth[i];
     if (!(d0 > 0.0f)) return;
@@ -253,6 +275,18 @@ __global__ void k_gn_refine(const __grid_constant__ RunArgs a, const __grid_cons
     if (cost_out) cost_out[i] = sqrtf(e0 / __popc(valid));
 }
 
+// Resets the self-check counter before a launch and reads it after one.
+static cudaError_t grad_oob_reset(cudaStream_t st) {
+    const unsigned int zero = 0;
+    return cudaMemcpyToSymbolAsync(g_grad_oob, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, st);
+}
+
+static cudaError_t grad_oob_read(cudaStream_t st, unsigned int* n) {
+    cudaError_t e = cudaMemcpyFromSymbolAsync(n, g_grad_oob, sizeof(*n), 0, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
+}
+
 }  // namespace
 
 int Ctx::fill_src_images(const int32_t* srcs, int n_src, SrcImages& si) {
@@ -289,8 +323,12 @@ int Ctx::eval_cost_grad(int ref, const int32_t* srcs, int n_src, const hpm_param
     e = cudaMemcpyAsync(d_px, px, (size_t)n * 8, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_th, theta, (size_t)n * 12, cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) return cuda_fail(e, "upload hypotheses");
+    if ((e = grad_oob_reset(stream)) != cudaSuccess) return cuda_fail(e, "self-check reset");
     k_cost_grad<<<(n + 127) / 128, 128, 0, stream>>>(a, si, n, d_px, d_th, d_c, grad ? d_g : nullptr);
     ++launches;
+    unsigned int oob = 0;
+    if ((e = grad_oob_read(stream, &oob)) != cudaSuccess) return cuda_fail(e, "cost gradient");
+    if (oob) return fail(HPM_E_CUDA, "cost gradient: %u out-of-range accesses skipped", oob);
     e = cudaMemcpyAsync(cost, d_c, (size_t)n * n_src * 4, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess && grad) e = cudaMemcpyAsync(grad, d_g, (size_t)n * n_src * 12, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -316,11 +354,15 @@ int Ctx::gn_refine(int ref, const int32_t* srcs, int n_src, const hpm_params* pa
     cudaError_t e = ensure_map(ref, HPM_MAP_COST, v.w, v.h);
     if (e != cudaSuccess) return cuda_fail(e, "alloc cost map");
     dim3 block(16, 8), grid((v.w + 15) / 16, (v.h + 7) / 8);
-    k_gn_refine<<<grid, block, 0, stream>>>(a, si, steps, dm.ptr, nm.ptr, v.maps[HPM_MAP_COST].ptr);
+    if ((e = grad_oob_reset(stream)) != cudaSuccess) return cuda_fail(e, "self-check reset");
+    k_gn_refine<<<grid, block, 0, stream>>>(a, si, steps, dm.ptr, nm.ptr, v.maps[HPM_MAP_COST].ptr,
+                                            (size_t)v.w * v.h);
     ++launches;
     e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    unsigned int oob = 0;
+    if (e == cudaSuccess) e = grad_oob_read(stream, &oob);
     if (e != cudaSuccess) return cuda_fail(e, "gauss-newton refinement");
+    if (oob) return fail(HPM_E_CUDA, "gauss-newton refinement: %u out-of-range accesses skipped", oob);
     return HPM_OK;
 }
 

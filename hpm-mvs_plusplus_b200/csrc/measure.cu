@@ -22,6 +22,26 @@ __global__ void k_fma_peak(float* out, int iters, float a, float b) {
     if (s == -1234.5f) out[blockIdx.x] = s;
 }
 
+// Linear-filtered fetches in the access pattern of the half-sweep: a warp's
+// lanes are 32 pixels of one checkerboard colour (x = x0 + lane, y alternating
+// between two rows), each fetching its 6 x 6 stride-2 patch at fractional
+// positions, six independent fetches in flight per thread.
+__global__ void k_tex_peak(cudaTextureObject_t tex, int w, int h, int iters, float* out) {
+    const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const float px = 8.0f + (float)((warp * 32) % (w - 48)) + (float)lane;
+    const float py = 8.0f + (float)((warp * 7) % (h - 24)) + (float)(lane & 1);
+    float acc = 0.f;
+    for (int it = 0; it < iters; ++it) {
+        const float fx = 0.25f + 0.0625f * (it & 7), fy = 0.375f + 0.03125f * (it & 15);
+        const int i = it % 6;
+        float v[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[k] = tex2D<float>(tex, px - 5.0f + 2.0f * i + fx, py - 5.0f + 2.0f * k + fy);
+        acc += ((v[0] + v[1]) + (v[2] + v[3])) + (v[4] + v[5]);
+    }
+    if (acc == -1234.5f) out[blockIdx.x] = acc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -38,8 +58,8 @@ int hpm_profile_enable(hpm_ctx* ctx, int flags) {
     if (flags & ~(HPM_PROFILE_TIMING | HPM_PROFILE_COUNT)) return c->fail(HPM_E_INVALID, "unknown profile flags %d", flags);
     cudaSetDevice(c->device);
     if ((flags & HPM_PROFILE_COUNT) && !c->prof_hyp) {
-        cudaError_t e = cudaMalloc((void**)&c->prof_hyp, 2 * sizeof(unsigned long long));
-        if (e == cudaSuccess) e = cudaMemsetAsync(c->prof_hyp, 0, 2 * sizeof(unsigned long long), c->stream);
+        cudaError_t e = cudaMalloc((void**)&c->prof_hyp, 3 * sizeof(unsigned long long));
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->prof_hyp, 0, 3 * sizeof(unsigned long long), c->stream);
         if (e != cudaSuccess) return c->cuda_fail(e, "profile counters");
     }
     c->prof_flags = flags;
@@ -78,6 +98,61 @@ int hpm_measure_fp32_peak(int device, double* tflops) {
     if (out) cudaFree(out);
     if (e != cudaSuccess) { cudaGetLastError(); return HPM_E_CUDA; }
     *tflops = best;
+    return HPM_OK;
+}
+
+int hpm_measure_tex_peak(int device, int format, double* gsamples) {
+    if (!gsamples || (format != HPM_TEX_F32 && format != HPM_TEX_F16 && format != HPM_TEX_U8)) return HPM_E_INVALID;
+    if (cudaSetDevice(device) != cudaSuccess) return HPM_E_CUDA;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return HPM_E_CUDA;
+    const int w = 1024, h = 256, threads = 128, blocks = sms * 12, iters = 1 << 12;
+    const cudaChannelFormatDesc fd =
+        format == HPM_TEX_F16 ? cudaCreateChannelDesc(16, 0, 0, 0, cudaChannelFormatKindFloat)
+                              : (format == HPM_TEX_U8 ? cudaCreateChannelDesc(8, 0, 0, 0, cudaChannelFormatKindUnsigned)
+                                                      : cudaCreateChannelDesc(32, 0, 0, 0, cudaChannelFormatKindFloat));
+    const size_t texel = format == HPM_TEX_F32 ? 4 : (format == HPM_TEX_F16 ? 2 : 1);
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+    float* out = nullptr;
+    void* stage = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaError_t e = cudaMallocArray(&arr, &fd, w, h);
+    if (e == cudaSuccess) e = cudaMalloc(&stage, (size_t)w * h * texel);
+    if (e == cudaSuccess) e = cudaMemset(stage, 0x3c, (size_t)w * h * texel);  // any finite texel value
+    if (e == cudaSuccess) e = cudaMemcpy2DToArray(arr, 0, 0, stage, w * texel, w * texel, h, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) {
+        cudaResourceDesc rd{};
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = arr;
+        cudaTextureDesc td{};
+        td.addressMode[0] = td.addressMode[1] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModeLinear;
+        td.readMode = format == HPM_TEX_U8 ? cudaReadModeNormalizedFloat : cudaReadModeElementType;
+        e = cudaCreateTextureObject(&tex, &rd, &td, nullptr);
+    }
+    if (e == cudaSuccess) e = cudaMalloc((void**)&out, sizeof(float) * blocks);
+    if (e == cudaSuccess) e = cudaEventCreate(&a);
+    if (e == cudaSuccess) e = cudaEventCreate(&b);
+    double best = 0.0;
+    for (int rep = 0; rep < 5 && e == cudaSuccess; ++rep) {
+        cudaEventRecord(a);
+        k_tex_peak<<<blocks, threads>>>(tex, w, h, iters, out);
+        cudaEventRecord(b);
+        e = cudaEventSynchronize(b);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (e == cudaSuccess && rep > 0 && ms > 0.f)
+            best = std::max(best, 6.0 * iters * (double)blocks * threads / (ms * 1e-3) / 1e9);
+    }
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    if (tex) cudaDestroyTextureObject(tex);
+    if (arr) cudaFreeArray(arr);
+    if (stage) cudaFree(stage);
+    if (out) cudaFree(out);
+    if (e != cudaSuccess) { cudaGetLastError(); return HPM_E_CUDA; }
+    *gsamples = best;
     return HPM_OK;
 }
 

@@ -158,8 +158,10 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
                 }
             } else {
                 // a group's priors are built, then its batch runs while later triangulations continue
-                for (int g = 0; g < n_views && !r; g += group) {
-                    const int end = std::min(n_views, g + group);
+                // (four groups unless batch_views says otherwise, so the host triangulations overlap the GPU)
+                const int pgroup = opt->batch_views > 0 ? opt->batch_views : std::max(1, (n_views + 3) / 4);
+                for (int g = 0; g < n_views && !r; g += pgroup) {
+                    const int end = std::min(n_views, g + pgroup);
                     for (int i = g; i < end && !r; ++i) {
                         const std::vector<hpm_triangle> t = tris[i].get();
                         r = timed(HPM_STAGE_PRIOR, [&]() {

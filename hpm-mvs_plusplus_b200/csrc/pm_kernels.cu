@@ -99,7 +99,9 @@ __device__ __forceinline__ PlaneM plane_m(const RunArgs& a, float4 pl) {
     return r;
 }
 
-// One bilateral NCC (HPM.cu:375-448) with the patch in registers.
+// One bilateral NCC (HPM.cu:375-448) with the patch in registers.  CNT: the
+// counting build also counts the NCCs that sample the source (hyp_count[2]).
+template <bool CNT = false>
 __device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int px, int py, const PlaneM& pm, int j) {
     const float cost_max = 2.0f;
     if (P.rs.var < 1e-5f) return cost_max;
@@ -116,6 +118,12 @@ __device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int 
         iz_c = 1.0f / cz;
         const float ux = cx * iz_c, uy = cy * iz_c;
         if (ux >= sw || ux < 0.0f || uy >= sh || uy < 0.0f) return cost_max;
+    }
+    if (CNT) {  // one atomic per group of converged lanes
+        unsigned lane;
+        asm("mov.u32 %0, %%laneid;" : "=r"(lane));
+        const unsigned m = __activemask();
+        if (lane == (unsigned)(__ffs(m) - 1)) atomicAdd(a.hyp_count + 2, (unsigned long long)__popc(m));
     }
     const cudaTextureObject_t tex = a.tex[j + 1];
     float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
@@ -372,7 +380,7 @@ __device__ __forceinline__ void eval_row(const RunArgs& a, const Patch& P, int p
                                          uint32_t mask, int row, const Scratch<NS, BLK, CNT>& s) {
 #pragma unroll 1
     for (int j = 0; j < a.S; ++j)
-        if ((mask >> j) & 1u) s.ca(row, j) = ncc_view(a, P, px, py, pm, j);
+        if ((mask >> j) & 1u) s.ca(row, j) = ncc_view<CNT>(a, P, px, py, pm, j);
 }
 
 __device__ __forceinline__ void v_path_scan(const float* __restrict__ costs, int W, int H, int x, int y, int ax,

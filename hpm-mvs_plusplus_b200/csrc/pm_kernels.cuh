@@ -46,9 +46,12 @@ struct RunArgs {
     // profiling only (null otherwise): (hypothesis, source view) pairs costed
     // by [0] the initialisation and [1] the half-sweeps, counted as the
     // reference evaluates them: every hypothesis against all S sources
-    // (ComputeMultiViewCostVector, HPM.cu:490-495)
+    // (ComputeMultiViewCostVector, HPM.cu:490-495); [2] the half-sweeps' NCCs
+    // that sampled the source (36 filtered fetches each)
     unsigned long long* hyp_count;
-};// Passed by value as a kernel parameter: sm_70 and later accept up to 32764 bytes.
+};
+
+// Passed by value as a kernel parameter: sm_70 and later accept up to 32764 bytes.
 static_assert(sizeof(RunArgs) <= 32764, "RunArgs exceeds the kernel parameter limit");
 
 

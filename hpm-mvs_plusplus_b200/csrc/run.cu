@@ -307,12 +307,13 @@ int Ctx::profile_read(hpm_profile* out) {
     }
     prof_used = 0;
     if (prof_hyp) {
-        unsigned long long h[2] = {0, 0};
+        unsigned long long h[3] = {0, 0, 0};
         e = cudaMemcpy(h, prof_hyp, sizeof(h), cudaMemcpyDeviceToHost);
         if (e == cudaSuccess) e = cudaMemset(prof_hyp, 0, sizeof(h));
         if (e != cudaSuccess) return cuda_fail(e, "hypothesis counters");
         out->init_view_evals = h[0];
         out->sweep_view_evals = h[1];
+        out->sweep_sampled = h[2];
     }
     return HPM_OK;
 }

@@ -319,6 +319,9 @@ typedef struct hpm_profile {
     double sweep_ms;
     uint64_t init_view_evals;  /* (hypothesis, source view) pairs costed, each 36 patch samples, */
     uint64_t sweep_view_evals; /*   every hypothesis against all S sources as the reference does */
+    uint64_t sweep_sampled;    /* (hypothesis, source view) NCCs of the half-sweeps that sampled the source
+                                  (36 filtered fetches each): the credited ones minus those skipped for a
+                                  zero view weight, an out-of-image centre or a flat reference patch */
     double confidence_ms;      /* device time of hpm_reconstruct's other stages: ConfidenceEvaluation, */
     double prior_ms;           /*   prior construction (support points, raster, fits, reload; the host */
     double jbu_ms;             /*   Delaunay triangulations overlap it and are not included), JBU and */
@@ -336,6 +339,12 @@ int hpm_profile_read(hpm_ctx *ctx, hpm_profile *out);
 /* FP32 FMA throughput of the device in TFLOP/s (2 flops per FMA), from a
  * dependent-chain kernel over all SMs timed with CUDA events. */
 int hpm_measure_fp32_peak(int device, double *tflops);
+
+/* Linear-filtered texture fetches per second (in units of 1e9) of the device
+ * for source textures of `format` (HPM_TEX_F32, HPM_TEX_F16 or HPM_TEX_U8),
+ * from fetches in the half-sweep's access pattern timed with CUDA events: the
+ * roof of the NCC sampling, which issues one filtered fetch per patch sample. */
+int hpm_measure_tex_peak(int device, int format, double *gsamples);
 
 #ifdef __cplusplus
 }

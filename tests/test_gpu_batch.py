@@ -148,14 +148,19 @@ def test_reconstruct_batched_where_exact_equals_sequential():
         assert got[2] == base[2], key
         for a, b in zip(got[0] + got[1], base[0] + base[1]):
             assert _same(a, b), key
-    # multi-geometry passes as Jacobi iterations: a different iteration, reported
+    # multi-geometry passes as Jacobi iterations: a different iteration, so different maps; it must reach
+    # the same accuracy against the rendered ground truth
     jac = res[(hpm_b200.RECON_BATCH_ALL, 0)]
-    agree = []
-    for d, db, nrm, nb in zip(jac[0], base[0], jac[1], base[1]):
+    agree, acc_j, acc_s = [], [], []
+    for v, d, db, nrm, nb in zip(sc.views, jac[0], base[0], jac[1], base[1]):
         ok = np.isfinite(d) & np.isfinite(db) & (db > 0)
         rel = np.abs(d - db) / np.maximum(np.abs(db), 1e-6)
         ang = np.degrees(np.arccos(np.clip((nrm * nb).sum(-1), -1, 1)))
         agree.append(float(((rel < 0.005) & (ang < 2.0))[ok].mean()))
+        gt = v.depth > 0
+        acc_j.append(float((np.abs(d - v.depth)[gt] < 0.01 * v.depth[gt]).mean()))
+        acc_s.append(float((np.abs(db - v.depth)[gt] < 0.01 * v.depth[gt]).mean()))
     print(f"Jacobi multi-geometry passes vs the sequential schedule: {np.round(agree, 3)} of pixels within "
-          f"0.5 % / 2 deg; points {jac[2]} vs {base[2]}")
-    assert min(agree) > 0.5
+          f"0.5 % / 2 deg; within 1 % of the true depth {np.mean(acc_j):.3f} vs {np.mean(acc_s):.3f}; "
+          f"points {jac[2]} vs {base[2]}")
+    assert abs(np.mean(acc_j) - np.mean(acc_s)) < 0.05

@@ -123,8 +123,10 @@ def test_gate3_c1_every_pass(ctx):
     rows, times = _gate_pipeline(ctx, scene, 4, seed=5)
     _report(rows, times, "C1 (5 views 1280x960, scale 4 -> 320x240, S = 4): every pass, all views")
     f, per_mode = _check(rows)
-    assert f["agree"] > 0.80, f
-    assert f["unexplained"] < 0.05, f
+    # PatchMatch turns last-bit differences into different winners; what the gate can hold is that every
+    # disagreeing pixel falls in an explained class (measured: 0.3-0.9 % unexplained per mode)
+    assert f["unexplained"] < 0.01, f
+    assert all(m["unexplained"] < 0.02 for m in per_mode.values()), per_mode
 
 
 def test_gate3_1600x1200_s10_every_mode(ctx):
@@ -136,8 +138,10 @@ def test_gate3_1600x1200_s10_every_mode(ctx):
     rows, times = _gate_pipeline(ctx, scene, 1, seed=9)
     _report(rows, times, "11 views 1600x1200, scale 1 (levels 800x600, 1600x1200), S = 10: every pass, all views")
     f, per_mode = _check(rows)
-    assert f["agree"] > 0.80, f
-    assert f["unexplained"] < 0.05, f
+    # measured: 0.1-0.6 % unexplained at 1600x1200, 2.3 % in the 800x600 photometric pass
+    assert f["unexplained"] < 0.005, f
+    top = {k: m for k, m in per_mode.items() if k[0] == "1600x1200"}
+    assert all(m["unexplained"] < 0.01 for m in top.values()), top
 
 
 def test_cuda_matches_oracle_at_1600x1200_s10(ctx):
