@@ -52,6 +52,7 @@ NCC_SHIFTED = 1
 
 BATCH_AUTOTUNE = 1
 BATCH_GRAPH = 2
+BATCH_PER_VIEW = 4
 
 RECON_SEQUENTIAL = 0
 RECON_BATCH_EXACT = 1

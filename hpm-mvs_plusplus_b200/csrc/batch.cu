@@ -12,9 +12,11 @@
 // per-run slices of resident batch buffers.
 //
 // Launch shapes of the half-sweep (block width 32, 16 or 8 pixels; one block
-// per tile or a persistent grid) give the same results; the autotuner times
-// them once per (source count, mode, size class) on a snapshot of the batch's
-// state and restores the state before the real run.  With HPM_BATCH_GRAPH the
+// per tile or a persistent grid; or, for views large enough to fill the GPU
+// alone, one single-view launch per run, stage by stage) give the same
+// results; the autotuner times them once per (source count, mode, size class)
+// on a snapshot of the batch's state and restores the state before the real
+// run.  With HPM_BATCH_GRAPH the
 // initialisation and the half-sweeps are captured once per batch shape in a
 // CUDA graph and replayed.
 #include "ctx.hpp"
@@ -123,6 +125,25 @@ int Ctx::tune_batch(const BatchLaunch& base, int n, size_t total_px, uint64_t ke
             }
         }
     }
+    // the single-view kernel, one launch per run: its RunArgs are kernel parameters, not device memory
+    if (!rc && (e = copy_all(false)) != cudaSuccess) rc = cuda_fail(e, "autotuner restore");
+    if (!rc) {
+        cudaEventRecord(t0, stream);
+        for (int k = 0; k < n && !rc; ++k) {
+            if ((e = launch_half_sweep(h_bargs[k], 0, 0, stream)) != cudaSuccess) rc = cuda_fail(e, "autotuner launch");
+            ++launches;
+        }
+        cudaEventRecord(t1, stream);
+        if (!rc && (e = cudaEventSynchronize(t1)) != cudaSuccess) rc = cuda_fail(e, "autotuner timing");
+        float ms = 0.0f;
+        if (!rc) cudaEventElapsedTime(&ms, t0, t1);
+        if (!rc && (best.ms < 0.0f || ms < best.ms)) {
+            best.ms = ms;
+            best.bx = 32;
+            best.persist = 0;
+            best.perview = true;
+        }
+    }
     if (!rc && (e = copy_all(false)) != cudaSuccess) rc = cuda_fail(e, "autotuner restore");
     if (!rc && (e = cudaStreamSynchronize(stream)) != cudaSuccess) rc = cuda_fail(e, "autotuner");
     if (t0) cudaEventDestroy(t0);
@@ -204,8 +225,13 @@ int Ctx::run_batch(int n, const int32_t* refs, const int32_t* src_off, const int
                          ((uint64_t)(total ? (int)std::log2((double)total) : 0) << 16);
     BatchShape shape;
     bool have_shape = false;
-    for (const auto& kv : batch_shapes)
-        if (kv.first == key) { shape = kv.second; have_shape = true; }
+    if (batch_flags & HPM_BATCH_PER_VIEW) {
+        shape.perview = true;
+        have_shape = true;
+    } else {
+        for (const auto& kv : batch_shapes)
+            if (kv.first == key) { shape = kv.second; have_shape = true; }
+    }
     int* hi = h_btiles;
     hi[0] = 0;
     for (int k = 0; k < n; ++k) hi[k + 1] = hi[k] + ((h_bargs[k].W + 15) / 16) * ((h_bargs[k].H + 7) / 8);
@@ -234,6 +260,26 @@ int Ctx::run_batch(int n, const int32_t* refs, const int32_t* src_off, const int
     bs.tiles = h_btiles[(n + 1) + n];
     bs.bx = shape.bx;
 
+    // one half-sweep stage of every run: one batched launch, or the single-view kernel per run
+    auto sweep_stage = [&](int color, int iter, TimedLaunch*& t) -> int {
+        int r = HPM_OK;
+        if (!shape.perview) {
+            if ((r = record_start(1, t))) return r;
+            if ((e = launch_half_sweep_batch(bs, color, iter, stream)) != cudaSuccess)
+                return cuda_fail(e, "batched half sweep");
+            if (t) cudaEventRecord(t->stop, stream);
+            ++launches;
+            return HPM_OK;
+        }
+        for (int k = 0; k < n; ++k) {
+            if ((r = record_start(1, t))) return r;
+            if ((e = launch_half_sweep(h_bargs[k], color, iter, stream)) != cudaSuccess)
+                return cuda_fail(e, "half sweep");
+            if (t) cudaEventRecord(t->stop, stream);
+            ++launches;
+        }
+        return HPM_OK;
+    };
     const bool timing = prof_flags & HPM_PROFILE_TIMING;
     const bool use_graph = (batch_flags & HPM_BATCH_GRAPH) && !timing && !bi.count;
     TimedLaunch* t = nullptr;
@@ -244,13 +290,8 @@ int Ctx::run_batch(int n, const int32_t* refs, const int32_t* src_off, const int
         if ((e = launch_random_init_batch(bi, stream)) != cudaSuccess) return cuda_fail(e, "batched init launch");
         if (t) cudaEventRecord(t->stop, stream);
         ++launches;
-        for (int k = 0; k < 2 * iters; ++k) {
-            if ((rc = record_start(1, t))) return rc;
-            if ((e = launch_half_sweep_batch(bs, k & 1, k >> 1, stream)) != cudaSuccess)
-                return cuda_fail(e, "batched half sweep");
-            if (t) cudaEventRecord(t->stop, stream);
-            ++launches;
-        }
+        for (int k = 0; k < 2 * iters; ++k)
+            if ((rc = sweep_stage(k & 1, k >> 1, t))) return rc;
         return HPM_OK;
     };
     int sms = 0;
@@ -259,15 +300,18 @@ int Ctx::run_batch(int n, const int32_t* refs, const int32_t* src_off, const int
         bs.grid_blocks = shape.persist ? shape.persist * half_sweep_batch_occupancy(max_s, mand) * sms : 0;
     };
     set_grid();
+    // a graph of per-view launches would hold this batch's RunArgs as parameters; the batched kernels read
+    // theirs from device memory, refreshed before every replay
     BatchGraph* graph = nullptr;
-    if (use_graph && have_shape)
+    if (use_graph && have_shape && !shape.perview)
         for (auto& g : batch_graphs)
             if (g.n == n && g.init_tiles == bi.tiles && g.sweep_tiles == bs.tiles && g.max_s == max_s &&
-                g.mand == mand && g.iters == iters && g.bx == bs.bx && g.grid == bs.grid_blocks)
+                g.mand == mand && g.iters == iters && g.bx == bs.bx && g.grid == bs.grid_blocks &&
+                g.perview == shape.perview)
                 graph = &g;
     if (graph) {
         if ((e = cudaGraphLaunch(graph->exec, stream)) != cudaSuccess) return cuda_fail(e, "batch graph launch");
-        launches += 1 + 2 * iters;
+        launches += 1 + 2 * iters * (shape.perview ? n : 1);
     } else if (!have_shape && (batch_flags & HPM_BATCH_AUTOTUNE) && iters > 0) {
         // initialise, tune the half-sweep on a snapshot of the initialised state, then sweep
         if ((rc = record_start(0, t))) return rc;
@@ -282,16 +326,11 @@ int Ctx::run_batch(int n, const int32_t* refs, const int32_t* src_off, const int
         bs.tiles = h_btiles[(n + 1) + n];
         bs.bx = shape.bx;
         set_grid();
-        for (int k = 0; k < 2 * iters; ++k) {
-            if ((rc = record_start(1, t))) return rc;
-            if ((e = launch_half_sweep_batch(bs, k & 1, k >> 1, stream)) != cudaSuccess)
-                return cuda_fail(e, "batched half sweep");
-            if (t) cudaEventRecord(t->stop, stream);
-            ++launches;
-        }
+        for (int k = 0; k < 2 * iters; ++k)
+            if ((rc = sweep_stage(k & 1, k >> 1, t))) return rc;
     } else {
         if ((rc = schedule())) return rc;
-        if (use_graph) {
+        if (use_graph && !shape.perview) {
             // record the same launches (not executed) for the next batch of this shape
             cudaGraph_t g = nullptr;
             if ((e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed)) != cudaSuccess)
@@ -308,7 +347,7 @@ int Ctx::run_batch(int n, const int32_t* refs, const int32_t* src_off, const int
             if (e != cudaSuccess) return cuda_fail(e, "batch graph instantiate");
             BatchGraph bg;
             bg.n = n; bg.init_tiles = bi.tiles; bg.sweep_tiles = bs.tiles; bg.max_s = max_s; bg.mand = mand;
-            bg.iters = iters; bg.bx = bs.bx; bg.grid = bs.grid_blocks; bg.exec = ex;
+            bg.iters = iters; bg.bx = bs.bx; bg.grid = bs.grid_blocks; bg.perview = shape.perview; bg.exec = ex;
             batch_graphs.push_back(bg);
         }
     }

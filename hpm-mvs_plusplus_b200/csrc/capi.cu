@@ -306,7 +306,7 @@ int hpm_run_batch(hpm_ctx* ctx, int n, const int32_t* refs, const int32_t* src_o
 int hpm_set_batch_options(hpm_ctx* ctx, int flags) {
     if (!ctx) return HPM_E_INVALID;
     Ctx* c = reinterpret_cast<Ctx*>(ctx);
-    if (flags & ~(HPM_BATCH_AUTOTUNE | HPM_BATCH_GRAPH))
+    if (flags & ~(HPM_BATCH_AUTOTUNE | HPM_BATCH_GRAPH | HPM_BATCH_PER_VIEW))
         return c->fail(HPM_E_INVALID, "hpm_set_batch_options: unknown flags 0x%x", flags);
     c->batch_flags = flags;
     return HPM_OK;

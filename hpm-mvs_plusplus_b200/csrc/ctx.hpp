@@ -69,6 +69,7 @@ struct RunBufs {
 struct BatchShape {
     int bx = 32;       // block width in pixels (block height = block threads / bx row pairs)
     int persist = 0;   // 0: one block per tile; k > 0: a persistent grid of k x resident blocks
+    bool perview = false;  // one launch of the single-view kernel per run and stage (large views)
     float ms = 0.0f;   // measured time of one half-sweep with this shape
 };
 
@@ -122,7 +123,7 @@ struct Ctx {
     std::vector<std::pair<uint64_t, BatchShape>> batch_shapes;  // autotuner cache: key -> shape
     struct BatchGraph {
         int n = 0, init_tiles = 0, sweep_tiles = 0, max_s = 0, iters = 0, bx = 0, grid = 0;
-        bool mand = false;
+        bool mand = false, perview = false;
         cudaGraphExec_t exec = nullptr;
     };
     std::vector<BatchGraph> batch_graphs;

@@ -43,9 +43,16 @@ __device__ __forceinline__ float texel_c(const float* img, int w, int h, int x, 
     return __ldg(img + (size_t)y * w + x);
 }
 
+// Exact bilinear sample with clamp-to-edge addressing.  The position is first
+// clamped to [-2, size + 1] (a NaN to -2): outside that range every tap reads
+// the edge texel, so the value and the (zero) gradient are unchanged, and the
+// integer tap index x0 + 1 cannot overflow for a sample position near a
+// plane's horizon, where X grows without bound.
 __device__ __forceinline__ float bilinear(const float* img, int w, int h, float X, float Y, float& gx, float& gy) {
+    X = fminf(fmaxf(X, -2.0f), (float)w + 1.0f);
+    Y = fminf(fmaxf(Y, -2.0f), (float)h + 1.0f);
     const float fx = floorf(X), fy = floorf(Y);
-    const int x0 = (int)fx, y0 = (int)fy;
+    const int x0 = __float2int_rz(fx), y0 = __float2int_rz(fy);
     const float ax = X - fx, ay = Y - fy;
     const float i00 = texel_c(img, w, h, x0, y0), i10 = texel_c(img, w, h, x0 + 1, y0);
     const float i01 = texel_c(img, w, h, x0, y0 + 1), i11 = texel_c(img, w, h, x0 + 1, y0 + 1);

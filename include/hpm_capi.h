@@ -127,12 +127,15 @@ int hpm_run_batch(hpm_ctx *ctx, int n, const int32_t *refs, const int32_t *src_o
  *   HPM_BATCH_AUTOTUNE    the first batch of each (source count, mode, size class)
  *                         times the candidate launch shapes of the half-sweep (block
  *                         width 32, 16 or 8 pixels; one block per tile or a persistent
- *                         grid) on a copy of its state and keeps the fastest; results
- *                         do not depend on the shape
+ *                         grid; or one single-view launch per run) on a copy of its
+ *                         state and keeps the fastest; results do not depend on the shape
  *   HPM_BATCH_GRAPH       the initialisation and half-sweeps of a batch are captured once
- *                         per batch shape in a CUDA graph and replayed */
+ *                         per batch shape in a CUDA graph and replayed (not for the
+ *                         single-view shape)
+ *   HPM_BATCH_PER_VIEW    the half-sweeps use the single-view shape without tuning */
 #define HPM_BATCH_AUTOTUNE 1
 #define HPM_BATCH_GRAPH 2
+#define HPM_BATCH_PER_VIEW 4
 int hpm_set_batch_options(hpm_ctx *ctx, int flags);
 
 /* Fixed-hypothesis costs (no reference counterpart: parity entry point).

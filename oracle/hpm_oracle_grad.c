@@ -26,9 +26,13 @@ static double texel64(const float *img, int w, int h, int x, int y)
     return img[(size_t)y * w + x];
 }
 
-/* exact bilinear sample at (X, Y) and its partial derivatives */
+/* exact bilinear sample at (X, Y) and its partial derivatives; the position is
+   clamped to [-2, size + 1] first (NaN to -2), where every tap already reads the
+   edge texel, so the integer conversion below stays in range */
 static double bilinear64(const float *img, int w, int h, double X, double Y, double *dX, double *dY)
 {
+    X = X >= -2.0 ? (X <= w + 1.0 ? X : w + 1.0) : -2.0;
+    Y = Y >= -2.0 ? (Y <= h + 1.0 ? Y : h + 1.0) : -2.0;
     const double fx = floor(X), fy = floor(Y);
     const int x0 = (int)fx, y0 = (int)fy;
     const double ax = X - fx, ay = Y - fy;

@@ -89,7 +89,10 @@ def test_batch_prior_mode_and_graph_replay(scene):
     srcs = [[j for j, _ in p] for p in scene.pairs]
     refs = list(range(6))
     out = []
-    for flags, reps in ((0, 1), (hpm_b200.BATCH_AUTOTUNE, 1), (hpm_b200.BATCH_GRAPH, 3)):
+    # the single-view shape (one launch per run and stage) must give the same maps; with it the graph
+    # option is ignored, so a second batch re-launches
+    for flags, reps in ((0, 1), (hpm_b200.BATCH_AUTOTUNE, 1), (hpm_b200.BATCH_GRAPH, 3),
+                        (hpm_b200.BATCH_PER_VIEW, 1), (hpm_b200.BATCH_PER_VIEW | hpm_b200.BATCH_GRAPH, 2)):
         with hpm_b200.Context(0) as ctx:
             ctx.set_batch_options(flags)
             cams = _load(ctx, scene)
@@ -163,4 +166,5 @@ def test_reconstruct_batched_where_exact_equals_sequential():
     print(f"Jacobi multi-geometry passes vs the sequential schedule: {np.round(agree, 3)} of pixels within "
           f"0.5 % / 2 deg; within 1 % of the true depth {np.mean(acc_j):.3f} vs {np.mean(acc_s):.3f}; "
           f"points {jac[2]} vs {base[2]}")
-    assert abs(np.mean(acc_j) - np.mean(acc_s)) < 0.05
+    # the Jacobi schedule may differ either way; it must not lose more than 5 points of accuracy
+    assert np.mean(acc_j) > np.mean(acc_s) - 0.05
