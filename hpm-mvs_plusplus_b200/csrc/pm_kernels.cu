@@ -128,31 +128,40 @@ __device__ __forceinline__ float ncc_view(const RunArgs& a, const Patch& P, int 
     const cudaTextureObject_t tex = a.tex[j + 1];
     float s_s = 0.f, s_ss = 0.f, s_rs = 0.f;
     float vshift = 0.0f;  // shifted moments: the source patch relative to its first sample
+    // two patch columns (12 fetches) are issued before their moments are summed: more fetches in
+    // flight per warp at the same register budget; the summation order is the oracle's
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        const float x = (float)(px - kPatchRadius + kPatchStep * i);
-        float v[6];
+    for (int i0 = 0; i0 < 6; i0 += 2) {
+        float v[2][6];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const float y = (float)(py - kPatchRadius + kPatchStep * k);
-            const float qx = hpm_fma(H[0], x, hpm_fma(H[1], y, H[2]));
-            const float qy = hpm_fma(H[3], x, hpm_fma(H[4], y, H[5]));
-            const float qz = hpm_fma(H[6], x, hpm_fma(H[7], y, H[8]));
-            const float iz = hpm_recip_near(qz, iz_c);
-            v[k] = tex2D<float>(tex, hpm_fma(qx, iz, 0.5f), hpm_fma(qy, iz, 0.5f));
+        for (int g = 0; g < 2; ++g) {
+            const float x = (float)(px - kPatchRadius + kPatchStep * (i0 + g));
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const float y = (float)(py - kPatchRadius + kPatchStep * k);
+                const float qx = hpm_fma(H[0], x, hpm_fma(H[1], y, H[2]));
+                const float qy = hpm_fma(H[3], x, hpm_fma(H[4], y, H[5]));
+                const float qz = hpm_fma(H[6], x, hpm_fma(H[7], y, H[8]));
+                const float iz = hpm_recip_near(qz, iz_c);
+                v[g][k] = tex2D<float>(tex, hpm_fma(qx, iz, 0.5f), hpm_fma(qy, iz, 0.5f));
+            }
         }
-        if (i == 0 && a.ncc_shift) vshift = v[0];
-        float r_s = 0.f, r_ss = 0.f, r_rs = 0.f;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const float2 w = P.p[i * 6 + k];
-            const float vk = v[k] - vshift;
-            const float ws = w.x * vk;
-            r_s += ws;
-            r_ss = hpm_fma(ws, vk, r_ss);
-            r_rs = hpm_fma(w.y, vk, r_rs);
+        for (int g = 0; g < 2; ++g) {
+            const int i = i0 + g;
+            if (i == 0 && a.ncc_shift) vshift = v[0][0];
+            float r_s = 0.f, r_ss = 0.f, r_rs = 0.f;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const float2 w = P.p[i * 6 + k];
+                const float vk = v[g][k] - vshift;
+                const float ws = w.x * vk;
+                r_s += ws;
+                r_ss = hpm_fma(ws, vk, r_ss);
+                r_rs = hpm_fma(w.y, vk, r_rs);
+            }
+            s_s += r_s; s_ss += r_ss; s_rs += r_rs;
         }
-        s_s += r_s; s_ss += r_ss; s_rs += r_rs;
     }
     s_s *= P.rs.inv_w; s_ss *= P.rs.inv_w; s_rs *= P.rs.inv_w;
     const float var_s = s_ss - s_s * s_s;
