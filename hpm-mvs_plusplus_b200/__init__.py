@@ -43,7 +43,8 @@ EXPORTED_SYMBOLS = (
     "hpm_jbu", "hpm_jbu_maps", "hpm_confidence_eval", "hpm_fuse", "hpm_support_points", "hpm_delaunay",
     "hpm_prior_from_triangles", "hpm_build_prior", "hpm_get_prior", "hpm_set_image", "hpm_prepare_level",
     "hpm_get_level", "hpm_reconstruct", "hpm_get_points", "hpm_get_stream", "hpm_profile_enable",
-    "hpm_profile_read", "hpm_measure_fp32_peak", "hpm_eval_costs_noalloc", "hpm_eval_cost_grad", "hpm_gn_refine",
+    "hpm_profile_read", "hpm_measure_fp32_peak", "hpm_eval_costs_noalloc", "hpm_eval_cost_grad",
+    "hpm_eval_cost_grad_device", "hpm_gn_refine",
     "hpm_set_texture_format", "hpm_run_batch", "hpm_set_batch_options", "hpm_set_ncc_mode", "hpm_measure_tex_peak",
 )
 
@@ -209,6 +210,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.hpm_eval_costs_noalloc.argtypes = lib.hpm_eval_costs.argtypes
     lib.hpm_eval_cost_grad.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int, vp,
                                        vp, vp, vp]
+    lib.hpm_eval_cost_grad_device.argtypes = lib.hpm_eval_cost_grad.argtypes
     lib.hpm_gn_refine.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.POINTER(Params), ctypes.c_int,
                                   ctypes.c_int]
     lib.hpm_set_address_mode.argtypes = [vp, ctypes.c_int]
@@ -400,6 +402,26 @@ class Context:
         self._check(self.lib.hpm_eval_cost_grad(self.h, ref, _ptr(s), len(s), ctypes.byref(params), p.shape[0],
                                                 _ptr(p), _ptr(th), _ptr(cost), _ptr(grad) if with_grad else None),
                     "hpm_eval_cost_grad")
+        return cost, grad
+
+    def eval_cost_grad_tensors(self, ref: int, srcs: Sequence[int], params: Params, px, theta, with_grad: bool = True):
+        """eval_cost_grad on CUDA tensors of the context's GPU (hpm_eval_cost_grad_device): px (n, 2) int32,
+        theta (n, 3) float32 -> cost (n, S) and grad (n, S, 3) float32 tensors; no host copies.  The context's
+        stream waits for torch's current stream first."""
+        import torch
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        p = px.to(torch.int32).reshape(-1, 2).contiguous()
+        th = theta.to(torch.float32).reshape(-1, 3).contiguous()
+        n = p.shape[0]
+        cost = torch.empty((n, len(s)), dtype=torch.float32, device=th.device)
+        grad = torch.empty((n, len(s), 3), dtype=torch.float32, device=th.device) if with_grad else None
+        stream = torch.cuda.ExternalStream(self.stream_handle(), device=th.device)
+        stream.wait_stream(torch.cuda.current_stream(th.device))
+        self._check(self.lib.hpm_eval_cost_grad_device(
+            self.h, ref, _ptr(s), len(s), ctypes.byref(params), n, ctypes.c_void_p(p.data_ptr()),
+            ctypes.c_void_p(th.data_ptr()), ctypes.c_void_p(cost.data_ptr()),
+            ctypes.c_void_p(grad.data_ptr()) if with_grad else None), "hpm_eval_cost_grad_device")
+        # the call returned after its kernel finished; keep the inputs alive until then
         return cost, grad
 
     def gn_refine(self, ref: int, srcs: Sequence[int], params: Params, depth_kind: int = MAP_DEPTH_GEOM,

@@ -7,8 +7,8 @@ camera frame (nz = -sqrt(1 - nx^2 - ny^2)); the result is the (n, S) tensor of
 per-view costs.  The forward pass asks the library for the costs and their
 gradients in one call (the adjoint kernel recomputes the warped samples); the
 backward pass contracts the stored (n, S, 3) Jacobian with the incoming
-gradient.  Host tensors are exchanged with the library; the costs are computed
-on the context's GPU.
+gradient.  CUDA tensors stay on the device (hpm_eval_cost_grad_device); host
+tensors go through hpm_eval_cost_grad.
 """
 from __future__ import annotations
 
@@ -19,10 +19,16 @@ import torch
 class NCCCost(torch.autograd.Function):
     @staticmethod
     def forward(fctx, theta: torch.Tensor, hctx, ref: int, srcs, params, px):
+        if theta.is_cuda:
+            p = px if torch.is_tensor(px) else torch.as_tensor(np.asarray(px), device=theta.device)
+            cost, grad = hctx.eval_cost_grad_tensors(ref, srcs, params, p.to(theta.device), theta.detach())
+            fctx.save_for_backward(grad)
+            return cost.to(theta.dtype)
         th = theta.detach().to("cpu", torch.float32).numpy()
-        cost, grad = hctx.eval_cost_grad(ref, srcs, params, np.asarray(px), th, with_grad=True)
-        fctx.save_for_backward(torch.from_numpy(grad).to(theta.device))
-        return torch.from_numpy(cost).to(device=theta.device, dtype=theta.dtype)
+        p = px.cpu().numpy() if torch.is_tensor(px) else np.asarray(px)
+        cost, grad = hctx.eval_cost_grad(ref, srcs, params, p, th, with_grad=True)
+        fctx.save_for_backward(torch.from_numpy(grad))
+        return torch.from_numpy(cost).to(dtype=theta.dtype)
 
     @staticmethod
     def backward(fctx, grad_out: torch.Tensor):

@@ -176,6 +176,8 @@ struct Ctx {
     int fill_src_images(const int32_t* srcs, int n_src, SrcImages& si);
     int eval_cost_grad(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n, const int32_t* px,
                        const float* theta, float* cost, float* grad);
+    int eval_cost_grad_device(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n,
+                              const int32_t* d_px, const float* d_theta, float* d_cost, float* d_grad);
     int gn_refine(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int depth_kind, int steps);
     int eval_costs(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n, const int32_t* px,
                    const float* planes, float* out);

@@ -343,6 +343,29 @@ int Ctx::eval_cost_grad(int ref, const int32_t* srcs, int n_src, const hpm_param
     return HPM_OK;
 }
 
+int Ctx::eval_cost_grad_device(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int n,
+                               const int32_t* d_px, const float* d_theta, float* d_cost, float* d_grad) {
+    cudaSetDevice(device);
+    if (n < 0 || (n > 0 && (!d_px || !d_theta || !d_cost)))
+        return fail(HPM_E_INVALID, "hpm_eval_cost_grad_device: bad arguments");
+    RunArgs a;
+    int rc = fill_run_args(ref, srcs, n_src, params, a);
+    if (rc) return rc;
+    SrcImages si{};
+    if ((rc = fill_src_images(srcs, n_src, si))) return rc;
+    if (n == 0) return HPM_OK;
+    cudaError_t e;
+    if ((e = grad_oob_reset(stream)) != cudaSuccess) return cuda_fail(e, "self-check reset");
+    // pixels outside the reference image are skipped and counted by the kernel (no host copy to check them)
+    k_cost_grad<<<(n + 127) / 128, 128, 0, stream>>>(a, si, n, d_px, d_theta, d_cost, d_grad);
+    ++launches;
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "cost gradient launch");
+    unsigned int oob = 0;
+    if ((e = grad_oob_read(stream, &oob)) != cudaSuccess) return cuda_fail(e, "cost gradient");
+    if (oob) return fail(HPM_E_INVALID, "cost gradient: %u pixels or samples outside their images skipped", oob);
+    return HPM_OK;
+}
+
 int Ctx::gn_refine(int ref, const int32_t* srcs, int n_src, const hpm_params* params, int depth_kind, int steps) {
     cudaSetDevice(device);
     if (steps < 0 || steps > 100) return fail(HPM_E_INVALID, "steps must be 0..100");
@@ -381,6 +404,13 @@ int hpm_eval_cost_grad(hpm_ctx* ctx, int ref, const int32_t* srcs, int n_src, co
                        const int32_t* px, const float* theta, float* cost, float* grad) {
     if (!ctx) return HPM_E_INVALID;
     return reinterpret_cast<hpm::Ctx*>(ctx)->eval_cost_grad(ref, srcs, n_src, params, n, px, theta, cost, grad);
+}
+
+int hpm_eval_cost_grad_device(hpm_ctx* ctx, int ref, const int32_t* srcs, int n_src, const hpm_params* params,
+                              int n, const int32_t* d_px, const float* d_theta, float* d_cost, float* d_grad) {
+    if (!ctx) return HPM_E_INVALID;
+    return reinterpret_cast<hpm::Ctx*>(ctx)->eval_cost_grad_device(ref, srcs, n_src, params, n, d_px, d_theta, d_cost,
+                                                                   d_grad);
 }
 
 int hpm_gn_refine(hpm_ctx* ctx, int ref, const int32_t* srcs, int n_src, const hpm_params* params, int depth_kind,

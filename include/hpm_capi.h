@@ -167,6 +167,14 @@ int hpm_eval_costs_noalloc(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src
 int hpm_eval_cost_grad(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, const hpm_params *params, int n,
                        const int32_t *px, const float *theta, float *cost, float *grad);
 
+/* hpm_eval_cost_grad on device buffers: px, theta, cost and grad are device
+ * pointers of the context's GPU, read and written on the context's stream
+ * (hpm_get_stream); the caller orders its own producers before the call.  The
+ * call returns when the kernel has finished.  A pixel outside the reference
+ * image is skipped and the call returns HPM_E_INVALID. */
+int hpm_eval_cost_grad_device(hpm_ctx *ctx, int ref, const int32_t *srcs, int n_src, const hpm_params *params, int n,
+                              const int32_t *d_px, const float *d_theta, float *d_cost, float *d_grad);
+
 /* Gauss-Newton refinement of a view's resident planes (no counterpart in the
  * reference, where refinement is PlaneHypothesisRefinement's random
  * perturbations, HPM.cu:765-841): `steps` damped Gauss-Newton steps per pixel

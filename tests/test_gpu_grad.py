@@ -98,6 +98,41 @@ def test_autograd_function(small_scene, loaded):
     assert np.allclose(th.grad.numpy(), expect, rtol=1e-5, atol=1e-6)
 
 
+def test_autograd_function_on_device_tensors(small_scene, loaded):
+    """CUDA tensors take the device entry point: the same costs and Jacobian as the host path, bit for bit,
+    and the backward pass stays on the GPU."""
+    torch = pytest.importorskip("torch")
+    from hpm_b200.autograd import NCCCost
+
+    ctx, cams, grays = loaded
+    v0 = small_scene.views[0]
+    srcs = [j for j, _ in small_scene.pairs[0]]
+    params = hpm_b200.Params.make(len(srcs) + 1, *hpm_b200.widened_range(cams[0]))
+    rng = np.random.default_rng(14)
+    ys, xs = np.nonzero(v0.depth > 0)
+    pick = rng.choice(len(xs), 256, replace=False)
+    px = np.stack([xs[pick], ys[pick]], 1).astype(np.int32)
+    th_np = _jittered(v0, xs[pick], ys[pick], rng).astype(np.float32)
+    cost_h, jac_h = ctx.eval_cost_grad(0, srcs, params, px, th_np)
+    th = torch.tensor(th_np, device="cuda:0", requires_grad=True)
+    px_d = torch.tensor(px, device="cuda:0")
+    cost_d, jac_d = ctx.eval_cost_grad_tensors(0, srcs, params, px_d, th.detach())
+    assert cost_d.is_cuda and jac_d.is_cuda
+    assert np.array_equal(cost_d.cpu().numpy(), cost_h) and np.array_equal(jac_d.cpu().numpy(), jac_h)
+    wts = torch.rand(256, len(srcs), device="cuda:0")
+    cost = NCCCost.apply(th, ctx, 0, srcs, params, px_d)
+    assert cost.is_cuda
+    (cost * wts).sum().backward()
+    assert th.grad.is_cuda
+    expect = (wts.cpu().numpy()[..., None] * jac_h).sum(1)
+    assert np.allclose(th.grad.cpu().numpy(), expect, rtol=1e-5, atol=1e-6)
+    # a pixel outside the reference image is reported, not read
+    bad = px_d.clone()
+    bad[3, 0] = 10_000
+    with pytest.raises(hpm_b200.HPMError, match="outside"):
+        ctx.eval_cost_grad_tensors(0, srcs, params, bad, th.detach())
+
+
 def test_gauss_newton_lowers_depth_error(small_scene, loaded):
     ctx, cams, grays = loaded
     v0 = small_scene.views[0]
