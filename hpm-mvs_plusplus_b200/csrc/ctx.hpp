@@ -91,6 +91,8 @@ struct Ctx {
     uint32_t* sel = nullptr; size_t run_cap_sel = 0;
     uint32_t* rng = nullptr; size_t run_cap_rng = 0;
     float* conf = nullptr; size_t run_cap_conf = 0;
+    int* active_px = nullptr; size_t active_px_cap = 0;  // prior-mode compaction (k_prior_active)
+    int* active_n = nullptr; size_t active_n_cap = 0;
     float4* scaled = nullptr; size_t scaled_cap = 0;
     uint8_t* scratch = nullptr; size_t scratch_cap = 0;
     uint8_t* scan_state = nullptr; size_t scan_state_cap = 0;

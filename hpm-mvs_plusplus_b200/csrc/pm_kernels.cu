@@ -924,6 +924,53 @@ __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep(const 
                                     color, iter);
 }
 
+// Prior mode with work lists (RunArgs::active_px): thread x of a row pair takes the x-th pixel the
+// sweep updates, so the pixels that return at once (confident, or outside the prior mask) leave
+// whole warps idle instead of holding lanes of working ones.  Pixels of one colour read only the
+// other colour's state, so the mapping does not change any result.
+template <int NS, int BLK, bool CNT>
+__global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS) k_half_sweep_listed(const __grid_constant__ RunArgs a,
+                                                                                 int color, int iter) {
+    extern __shared__ float smem[];
+    const int pair = blockIdx.y * blockDim.y + threadIdx.y;
+    if (pair >= a.cover_pairs) return;
+    const int k = color * a.cover_pairs + pair;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= a.active_n[k]) return;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const Scratch<NS, BLK, CNT> s{ smem + tid };
+    sweep_pixel<NS, BLK, false, CNT>(a, s, a.active_px[(size_t)k * a.W + x], pair, color, iter);
+}
+
+// The pixels a prior-mode half-sweep updates (CheckerboardPropagation returns at once where
+// confidence > 0.3 or the prior mask is clear, HPM.cu:1352-1365): one warp per (row pair, colour)
+// writes their columns in increasing order and their count.
+__global__ void k_prior_active(const __grid_constant__ RunArgs a, int* __restrict__ out_px, int* __restrict__ out_n) {
+    const int pair = blockIdx.x, color = blockIdx.y, lane = threadIdx.x;
+    const int W = a.W, H = a.H;
+    int* row = out_px + ((size_t)color * a.cover_pairs + pair) * W;
+    int n = 0;
+    for (int x0 = 0; x0 < W; x0 += 32) {
+        const int px = x0 + lane;
+        const int py = 2 * pair + ((px & 1) ^ color);
+        bool act = false;
+        if (px < W && py < H) {
+            const int c = py * W + px;
+            act = !(a.conf[c] > 0.3) && a.pmask[c] != 0;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, act);
+        if (act) row[n + __popc(m & ((1u << lane) - 1u))] = px;
+        n += __popc(m);
+    }
+    if (lane == 0) out_n[color * a.cover_pairs + pair] = n;
+}
+
+cudaError_t launch_prior_active(const RunArgs& a, int* px, int* n, cudaStream_t st) {
+    if (a.cover_pairs <= 0) return cudaSuccess;
+    k_prior_active<<<dim3(a.cover_pairs, 2), 32, 0, st>>>(a, px, n);
+    return cudaGetLastError();
+}
+
 template <int NS, int BLK, bool MAND, bool CNT>
 __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS)
     k_half_sweep_batch(const RunArgs* __restrict__ args, const int* __restrict__ tile_start, int n, int color,
@@ -993,6 +1040,13 @@ static cudaError_t sweep_impl(const RunArgs& a, int color, int iter, cudaStream_
 #endif
     constexpr int BX = HPM_SWEEP_BX < BLK ? HPM_SWEEP_BX : BLK;
     dim3 block(BX, BLK / BX), grid((a.W + BX - 1) / BX, (a.cover_pairs + BLK / BX - 1) / (BLK / BX));
+    if (!MAND && a.active_px) {
+        auto kl = k_half_sweep_listed<NS, BLK, CNT>;
+        if ((e = cudaFuncSetAttribute(kl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm)) != cudaSuccess)
+            return e;
+        kl<<<grid, block, shm, st>>>(a, color, iter);
+        return cudaGetLastError();
+    }
     k<<<grid, block, shm, st>>>(a, color, iter);
     return cudaGetLastError();
 }

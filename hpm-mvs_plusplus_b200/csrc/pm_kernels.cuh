@@ -39,6 +39,10 @@ struct RunArgs {
     const uint8_t* canny;           // 0/255 edge map
     float* texture;                 // edge-density output
     const float4* scaled;           // hierarchy input map (scaled_cols x scaled_rows)
+    // prior mode: per colour and row pair, the columns of the pixels a half-sweep updates, compacted
+    // to the left (k_prior_active); null: every pixel of the colour is visited and skips itself
+    const int* active_px;           // [(colour * cover_pairs + pair) * W + k]
+    const int* active_n;            // [colour * cover_pairs + pair]
     hpm_params prm;
     int S, W, H, cover_pairs;
     uint64_t seed;
@@ -58,6 +62,9 @@ static_assert(sizeof(RunArgs) <= 32764, "RunArgs exceeds the kernel parameter li
 // Host launchers (pm_kernels.cu).  Return cudaError_t of the launch.
 cudaError_t launch_random_init(const RunArgs& a, cudaStream_t st);
 cudaError_t launch_half_sweep(const RunArgs& a, int color, int iter, cudaStream_t st);
+// Prior mode: the compacted columns of the pixels the half-sweeps update (W * cover_pairs ints and
+// cover_pairs counts per colour in px / n), for RunArgs::active_px / active_n.
+cudaError_t launch_prior_active(const RunArgs& a, int* px, int* n, cudaStream_t st);
 cudaError_t launch_export(const RunArgs& a, cudaStream_t st);
 // Fixed-hypothesis costs: out[k*S + j] for pixels px[2k], px[2k+1] and planes[k].
 cudaError_t launch_eval_costs(const RunArgs& a, int n, const int32_t* px, const float4* planes, float* out,

@@ -270,14 +270,29 @@ int Ctx::record_start(int kind, TimedLaunch*& slot) {
     return e == cudaSuccess ? HPM_OK : cuda_fail(e, "profiling event record");
 }
 
-int Ctx::launch_schedule(const RunArgs& a, int n_half_sweeps) {
+int Ctx::launch_schedule(const RunArgs& a0, int n_half_sweeps) {
     cudaError_t e;
     TimedLaunch* t = nullptr;
     int rc = record_start(0, t);
     if (rc) return rc;
-    if ((e = launch_random_init(a, stream)) != cudaSuccess) return cuda_fail(e, "init launch");
+    if ((e = launch_random_init(a0, stream)) != cudaSuccess) return cuda_fail(e, "init launch");
     if (t) cudaEventRecord(t->stop, stream);
     ++launches;
+    RunArgs a = a0;
+    const uint32_t mode = a0.prm.mode;
+    if ((mode & HPM_MODE_PRIOR) && !(mode & HPM_MODE_MAND) && n_half_sweeps > 0) {
+        // confidences and the prior mask do not change during a prior-mode run: the pixels its
+        // half-sweeps update are listed once, after the initialisation
+        const size_t rows = 2 * (size_t)a0.cover_pairs;
+        if ((e = ensure_buf(active_px, active_px_cap, rows * a0.W)) != cudaSuccess ||
+            (e = ensure_buf(active_n, active_n_cap, rows)) != cudaSuccess)
+            return cuda_fail(e, "alloc prior work lists");
+        if ((e = launch_prior_active(a0, active_px, active_n, stream)) != cudaSuccess)
+            return cuda_fail(e, "prior work lists");
+        ++launches;
+        a.active_px = active_px;
+        a.active_n = active_n;
+    }
     for (int k = 0; k < n_half_sweeps; ++k) {
         if ((rc = record_start(1, t))) return rc;
         if ((e = launch_half_sweep(a, k & 1, k >> 1, stream)) != cudaSuccess) return cuda_fail(e, "half sweep");
