@@ -219,6 +219,26 @@ int Ctx::run_batch(int n, const int32_t* refs, const int32_t* src_off, const int
         off += (size_t)views[r].w * views[r].h;
     }
 
+    // prior mode: work lists of every run (confidences and prior masks are fixed during the pass and the
+    // initialisation does not change them), computed before the launches that a graph may replay
+    const bool listed = prior && !mand && iters > 0;
+    if (listed) {
+        size_t words = 0;
+        for (int k = 0; k < n; ++k) words += 2 * (size_t)h_bargs[k].cover_pairs * (h_bargs[k].W + 1);
+        if ((e = ensure_dev(b_active, b_active_cap, words)) != cudaSuccess) return cuda_fail(e, "alloc prior work lists");
+        size_t w = 0;
+        for (int k = 0; k < n; ++k) {
+            RunArgs& a = h_bargs[k];
+            int* px = b_active + w;
+            int* cnt = px + 2 * (size_t)a.cover_pairs * a.W;
+            w += 2 * (size_t)a.cover_pairs * (a.W + 1);
+            if ((e = launch_prior_active(a, px, cnt, stream)) != cudaSuccess) return cuda_fail(e, "prior work lists");
+            ++launches;
+            a.active_px = px;
+            a.active_n = cnt;
+        }
+    }
+
     // tile tables: initialisation (16 x 8 pixel blocks), then the half-sweep's
     const int bt = half_sweep_block_threads(max_s);
     const uint64_t key = (uint64_t)max_s | ((uint64_t)mand << 8) |
@@ -254,6 +274,7 @@ int Ctx::run_batch(int n, const int32_t* refs, const int32_t* src_off, const int
     bi.max_s = max_s;
     bi.grid_blocks = 0;
     bi.mand = mand;
+    bi.listed = listed;
     bi.count = (prof_flags & HPM_PROFILE_COUNT) && prof_hyp;
     BatchLaunch bs = bi;
     bs.tile_start = d_btiles + (n + 1);

@@ -87,7 +87,7 @@ Ctx::~Ctx() {
     if (h_bargs) cudaFreeHost(h_bargs);
     if (h_btiles) cudaFreeHost(h_btiles);
     for (void* p : { (void*)planes, (void*)costs, (void*)pre_costs, (void*)sel, (void*)rng, (void*)conf,
-                     (void*)active_px, (void*)active_n,
+                     (void*)active_px, (void*)active_n, (void*)b_active,
                      (void*)scaled, (void*)scratch, (void*)scan_state, (void*)scan_work, (void*)points,
                      (void*)prior_small, (void*)prior_tris, (void*)prior_label, (void*)prior_work,
                      (void*)prior_unormal, (void*)canny_mag, (void*)canny_grad, (void*)canny_state })

@@ -93,6 +93,7 @@ struct Ctx {
     float* conf = nullptr; size_t run_cap_conf = 0;
     int* active_px = nullptr; size_t active_px_cap = 0;  // prior-mode compaction (k_prior_active)
     int* active_n = nullptr; size_t active_n_cap = 0;
+    int* b_active = nullptr; size_t b_active_cap = 0;    // the same for every run of a prior-mode batch
     float4* scaled = nullptr; size_t scaled_cap = 0;
     uint8_t* scratch = nullptr; size_t scratch_cap = 0;
     uint8_t* scan_state = nullptr; size_t scan_state_cap = 0;

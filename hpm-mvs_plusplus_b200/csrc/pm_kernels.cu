@@ -971,6 +971,29 @@ cudaError_t launch_prior_active(const RunArgs& a, int* px, int* n, cudaStream_t 
     return cudaGetLastError();
 }
 
+// The batched form of k_half_sweep_listed: tile t of run k maps to columns of that run's work lists.
+template <int NS, int BLK, bool CNT>
+__global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS)
+    k_half_sweep_batch_listed(const RunArgs* __restrict__ args, const int* __restrict__ tile_start, int n,
+                              int color, int iter) {
+    extern __shared__ float smem[];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const Scratch<NS, BLK, CNT> s{ smem + tid };
+    const int total = __ldg(tile_start + n);
+    for (int b = blockIdx.x; b < total; b += gridDim.x) {
+        const int k = batch_run_of(tile_start, n, b);
+        const RunArgs& a = args[k];
+        const int t = b - __ldg(tile_start + k);
+        const int tx = (a.W + blockDim.x - 1) / blockDim.x;
+        const int x = (t % tx) * blockDim.x + threadIdx.x;
+        const int pair = (t / tx) * blockDim.y + threadIdx.y;
+        if (pair >= a.cover_pairs) continue;
+        const int r = color * a.cover_pairs + pair;
+        if (x >= a.active_n[r]) continue;
+        sweep_pixel<NS, BLK, false, CNT>(a, s, a.active_px[(size_t)r * a.W + x], pair, color, iter);
+    }
+}
+
 template <int NS, int BLK, bool MAND, bool CNT>
 __global__ void __launch_bounds__(BLK, HPM_SWEEP_MIN_BLOCKS)
     k_half_sweep_batch(const RunArgs* __restrict__ args, const int* __restrict__ tile_start, int n, int color,
@@ -1067,7 +1090,7 @@ template <int NS, bool MAND, bool CNT>
 static cudaError_t sweep_batch_impl(const BatchLaunch& bl, int color, int iter, cudaStream_t st) {
     constexpr int BLK = block_threads<NS>();
     const size_t shm = sizeof(float) * Scratch<NS, BLK>::kWords * BLK;
-    auto k = k_half_sweep_batch<NS, BLK, MAND, CNT>;
+    auto k = (!MAND && bl.listed) ? k_half_sweep_batch_listed<NS, BLK, CNT> : k_half_sweep_batch<NS, BLK, MAND, CNT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     if (e != cudaSuccess) return e;
     const int grid = bl.grid_blocks > 0 && bl.grid_blocks < bl.tiles ? bl.grid_blocks : bl.tiles;

@@ -83,6 +83,7 @@ struct BatchLaunch {
     int grid_blocks;  // 0 or >= tiles: one block per tile; else a persistent grid of this many blocks
     int bx;           // half-sweep block width in pixels (32, 16 or 8); the initialisation uses 16 x 8
     bool mand;        // mandatory-consistency kernel
+    bool listed;      // prior mode with work lists (RunArgs::active_px of every run set)
     bool count;       // counting build (hyp_count of every run set)
 };
 
