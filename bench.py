@@ -336,6 +336,9 @@ def run_ours(args, scene, rank, world, local_rank):
     traffic = _ncu_traffic()
     # the unit that binds the half-sweep: the texture unit's linear filtering, one fetch per patch sample
     tex_peak = hb.measure_tex_peak(local_rank, hb.TEX_F32)
+    # the same fetches with every lane's patch at its own offset (up to +-16 px): the rate when the lanes of
+    # a warp sample under unrelated planes, as random refinement candidates do
+    tex_divergent = hb.measure_tex_rate(local_rank, hb.TEX_F32, 16.0)
     sampled_per_step = counted.sweep_sampled * SAMPLES_PER_NCC
     tex_achieved = sampled_per_step / (sweep_ms_per_step * 1e-3) / 1e9 if sweep_ms_per_step > 0 else None
     roofline = {
@@ -355,6 +358,10 @@ def run_ours(args, scene, rank, world, local_rank):
                     "peak_source": "hpm_measure_tex_peak: linear-filtered F32 fetches in the half-sweep's access "
                                    "pattern on this GPU",
                     "fetches_per_step": sampled_per_step,
+                    "divergent_lanes_rate": tex_divergent,
+                    "frac_of_divergent_rate": (tex_achieved / tex_divergent) if tex_achieved and tex_divergent else None,
+                    "divergent_source": "hpm_measure_tex_rate(jitter 16 px): the same fetches, each lane's patch moved "
+                                        "by its own random offset",
                     "note": "executed work: NCCs that sampled the source (zero-weight views, out-of-image centres "
                             "and flat reference patches skip sampling), 36 fetches each"},
         "fp32_executed": {"achieved": (sampled_per_step * ALGO_FLOPS_PER_EVAL / (sweep_ms_per_step * 1e-3) / 1e12)

@@ -46,6 +46,7 @@ EXPORTED_SYMBOLS = (
     "hpm_profile_read", "hpm_measure_fp32_peak", "hpm_eval_costs_noalloc", "hpm_eval_cost_grad",
     "hpm_eval_cost_grad_device", "hpm_gn_refine",
     "hpm_set_texture_format", "hpm_run_batch", "hpm_set_batch_options", "hpm_set_ncc_mode", "hpm_measure_tex_peak",
+    "hpm_measure_tex_rate",
 )
 
 NCC_PLAIN = 0
@@ -244,6 +245,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.hpm_profile_read.argtypes = [vp, ctypes.POINTER(Profile)]
     lib.hpm_measure_fp32_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.hpm_measure_tex_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.hpm_measure_tex_rate.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTED_SYMBOLS:
         getattr(lib, name)
     del i32, f
@@ -620,4 +622,15 @@ def measure_tex_peak(device: int = 0, fmt: int = TEX_F32) -> float:
     rc = lib.hpm_measure_tex_peak(device, fmt, ctypes.byref(out))
     if rc != 0:
         raise HPMError(f"hpm_measure_tex_peak failed ({rc})")
+    return out.value
+
+
+def measure_tex_rate(device: int = 0, fmt: int = TEX_F32, jitter: float = 0.0) -> float:
+    """Filtered fetches per second (1e9/s) with every lane's patch moved by up to +-jitter px
+    (hpm_measure_tex_rate)."""
+    lib = load_library()
+    out = ctypes.c_double()
+    rc = lib.hpm_measure_tex_rate(device, fmt, ctypes.c_float(jitter), ctypes.byref(out))
+    if rc != 0:
+        raise HPMError(f"hpm_measure_tex_rate failed ({rc})")
     return out.value

@@ -22,11 +22,20 @@ __global__ void k_fma_peak(float* out, int iters, float a, float b) {
     if (s == -1234.5f) out[blockIdx.x] = s;
 }
 
+__device__ __forceinline__ unsigned tex_probe_hash(unsigned x) {
+    x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+    return x;
+}
+
 // Linear-filtered fetches in the access pattern of the half-sweep: a warp's
 // lanes are 32 pixels of one checkerboard colour (x = x0 + lane, y alternating
 // between two rows), each fetching its 6 x 6 stride-2 patch at fractional
-// positions, six independent fetches in flight per thread.
-__global__ void k_tex_peak(cudaTextureObject_t tex, int w, int h, int iters, float* out) {
+// positions, six independent fetches in flight per thread.  With jitter > 0
+// every lane's patch is moved by its own offset, uniform in [-jitter, jitter]
+// pixels per axis and redrawn for every column of six fetches: the lanes of a
+// warp then sample apart, as they do when neighbouring pixels hold different
+// planes.  Coordinates outside the texture are clamped by the texture unit.
+__global__ void k_tex_peak(cudaTextureObject_t tex, int w, int h, int iters, float jitter, float* out) {
     const int lane = threadIdx.x & 31, warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const float px = 8.0f + (float)((warp * 32) % (w - 48)) + (float)lane;
     const float py = 8.0f + (float)((warp * 7) % (h - 24)) + (float)(lane & 1);
@@ -34,9 +43,16 @@ __global__ void k_tex_peak(cudaTextureObject_t tex, int w, int h, int iters, flo
     for (int it = 0; it < iters; ++it) {
         const float fx = 0.25f + 0.0625f * (it & 7), fy = 0.375f + 0.03125f * (it & 15);
         const int i = it % 6;
+        float jx = 0.f, jy = 0.f;
+        if (jitter > 0.f) {
+            const unsigned hv = tex_probe_hash((unsigned)(warp * 131 + lane) * 977u + (unsigned)(it / 6) * 7919u);
+            jx = jitter * ((float)(hv & 0xffffu) * (2.0f / 65535.0f) - 1.0f);
+            jy = jitter * ((float)(hv >> 16) * (2.0f / 65535.0f) - 1.0f);
+        }
         float v[6];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) v[k] = tex2D<float>(tex, px - 5.0f + 2.0f * i + fx, py - 5.0f + 2.0f * k + fy);
+        for (int k = 0; k < 6; ++k)
+            v[k] = tex2D<float>(tex, px + jx - 5.0f + 2.0f * i + fx, py + jy - 5.0f + 2.0f * k + fy);
         acc += ((v[0] + v[1]) + (v[2] + v[3])) + (v[4] + v[5]);
     }
     if (acc == -1234.5f) out[blockIdx.x] = acc;
@@ -102,7 +118,12 @@ int hpm_measure_fp32_peak(int device, double* tflops) {
 }
 
 int hpm_measure_tex_peak(int device, int format, double* gsamples) {
+    return hpm_measure_tex_rate(device, format, 0.0f, gsamples);
+}
+
+int hpm_measure_tex_rate(int device, int format, float jitter, double* gsamples) {
     if (!gsamples || (format != HPM_TEX_F32 && format != HPM_TEX_F16 && format != HPM_TEX_U8)) return HPM_E_INVALID;
+    if (!(jitter >= 0.0f && jitter <= 64.0f)) return HPM_E_INVALID;
     if (cudaSetDevice(device) != cudaSuccess) return HPM_E_CUDA;
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return HPM_E_CUDA;
@@ -137,7 +158,7 @@ int hpm_measure_tex_peak(int device, int format, double* gsamples) {
     double best = 0.0;
     for (int rep = 0; rep < 5 && e == cudaSuccess; ++rep) {
         cudaEventRecord(a);
-        k_tex_peak<<<blocks, threads>>>(tex, w, h, iters, out);
+        k_tex_peak<<<blocks, threads>>>(tex, w, h, iters, jitter, out);
         cudaEventRecord(b);
         e = cudaEventSynchronize(b);
         float ms = 0.f;

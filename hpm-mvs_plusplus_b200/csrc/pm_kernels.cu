@@ -329,7 +329,9 @@ __device__ __forceinline__ void init_pixel(const RunArgs& a, const Scratch<NS, B
 }
 
 template <int NS, int BLK, bool CNT>
-__global__ void __launch_bounds__(BLK) k_random_init(const __grid_constant__ RunArgs a) {
+// 3 blocks per SM (at most 168 registers): 12 warps, against 8 at the unbounded 174 registers; 1.5 ms
+// instead of 1.8 ms per 1600x1200 initialisation with 32 x 4 blocks
+__global__ void __launch_bounds__(BLK, 3) k_random_init(const __grid_constant__ RunArgs a) {
     extern __shared__ float smem[];
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const Scratch<NS, BLK, CNT> s{ smem + tid };
@@ -1046,7 +1048,7 @@ static cudaError_t init_impl(const RunArgs& a, cudaStream_t st) {
     auto k = k_random_init<NS, BLK, CNT>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     if (e != cudaSuccess) return e;
-    dim3 block(16, 8), grid((a.W + 15) / 16, (a.H + 7) / 8);
+    dim3 block(32, 4), grid((a.W + 31) / 32, (a.H + 3) / 4);
     k<<<grid, block, shm, st>>>(a);
     return cudaGetLastError();
 }

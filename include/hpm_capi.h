@@ -357,6 +357,12 @@ int hpm_measure_fp32_peak(int device, double *tflops);
  * roof of the NCC sampling, which issues one filtered fetch per patch sample. */
 int hpm_measure_tex_peak(int device, int format, double *gsamples);
 
+/* hpm_measure_tex_peak with the lanes of a warp apart: every lane's patch is
+ * moved by its own offset, uniform in [-jitter, jitter] pixels per axis
+ * (0 <= jitter <= 64) and redrawn for every six fetches, as when neighbouring
+ * pixels sample under different planes.  jitter = 0 is hpm_measure_tex_peak. */
+int hpm_measure_tex_rate(int device, int format, float jitter, double *gsamples);
+
 #ifdef __cplusplus
 }
 #endif
