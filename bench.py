@@ -223,8 +223,9 @@ def view_pixel_runs(w: int, h: int, scale: int, geom_iterations: int = 3) -> int
 def depth_accuracy(depths, scene, rel: float = 0.01):
     """Share of the rendered ground truth's valid pixels whose reconstructed depth lies within `rel`
     of it, over all views.  Maps smaller than the truth by an integer factor f (--initial-image-scale f)
-    are compared with the truth at the full-resolution pixel nearest to each map pixel's centre, f*x +
-    f/2; None when the sizes do not relate that way.  Computed after the timed steps from the maps the
+    are compared with the truth at full-resolution pixel (f*x, f*y): the level's camera is K scaled by
+    1/f (no half-pixel shift), so map pixel x looks along the ray of full-resolution pixel f*x.  None
+    when the sizes do not relate that way.  Computed after the timed steps from the maps the
     last step downloaded."""
     try:
         ok = hit = 0
@@ -234,7 +235,7 @@ def depth_accuracy(depths, scene, rel: float = 0.01):
                 f = gt.shape[0] // d.shape[0]
                 if f < 2 or gt.shape[0] != f * d.shape[0] or gt.shape[1] != f * d.shape[1]:
                     return None
-                gt = gt[f // 2::f, f // 2::f]
+                gt = gt[::f, ::f]
             m = gt > 0
             ok += int(m.sum())
             hit += int((np.abs(d[m] - gt[m]) <= rel * gt[m]).sum())

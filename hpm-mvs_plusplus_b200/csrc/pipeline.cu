@@ -135,7 +135,9 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
                 if (r) return r;
             }
             std::vector<std::future<std::vector<hpm_triangle>>> tris(n_views);
-            const int workers = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+            // two cores stay with the thread that feeds the GPU, so that it is not preempted by the workers
+            const unsigned hc = std::thread::hardware_concurrency();
+            const int workers = (int)std::max(1u, std::min(16u, hc > 3 ? hc - 2 : 1u));
             std::atomic<int> next{ 0 };
             std::vector<std::promise<std::vector<hpm_triangle>>> done(n_views);
             for (int i = 0; i < n_views; ++i) tris[i] = done[i].get_future();
