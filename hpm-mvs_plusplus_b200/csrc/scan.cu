@@ -35,6 +35,7 @@ namespace hpm {
 
 constexpr int kScanBlock = 1024;
 constexpr int kMaxScanIterations = 256;
+constexpr int kRoundsPerCheck = 4;  // fixed-point rounds launched between host reads of their flags
 // "not marked" value of marktime: the byte pattern 0x7f written by cudaMemset
 constexpr int32_t kUnmarked = 0x7F7F7F7F;
 
@@ -202,6 +203,17 @@ __global__ void k_last_combine(int32_t* __restrict__ last, const int32_t* __rest
         int32_t& v = last[(size_t)q * n_ngb + j];
         v = max(v, pre);
     }
+}
+
+// The marks of every source of the current view back to "not marked" (marktime) and -1
+// (marklast, confidence mode): one launch for all sources of a round, row j of the grid for
+// source j.
+__global__ void k_reset_marks(const ScanView* __restrict__ views, const int32_t* __restrict__ srcs, int with_last) {
+    const ScanView& vs = views[srcs[blockIdx.y]];
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= vs.W * vs.H) return;
+    vs.marktime[p] = kUnmarked;
+    if (with_last) vs.marklast[p] = -1;
 }
 
 template <int MODE>
@@ -458,7 +470,7 @@ int Ctx::consistency_scan(int mode, int n_views, const int32_t* src_off, const i
     const size_t nblocks_max = (max_pix + kScanBlock - 1) / kScanBlock;
     const size_t ng = std::max(1, max_ngb);
     const size_t wbytes = al(4 * max_pix * ng) + al(8 * max_pix * ng) + al(4 * max_pix * ng) + 5 * al(4 * max_pix) +
-                          al(max_pix) + al(4 * nblocks_max * ng) + al(64);
+                          al(max_pix) + al(4 * nblocks_max * ng) + al(64) + al(4 * kMaxScanIterations);
     e = ensure_dev(scan_work, scan_work_cap, wbytes);
     if (e != cudaSuccess) return cuda_fail(e, "alloc scan work");
     cur = scan_work;
@@ -472,8 +484,8 @@ int Ctx::consistency_scan(int mode, int n_views, const int32_t* src_off, const i
     int32_t* keep = reinterpret_cast<int32_t*>(carve(4 * max_pix));
     int32_t* offs = reinterpret_cast<int32_t*>(carve(4 * max_pix));
     int32_t* block_max = reinterpret_cast<int32_t*>(carve(4 * nblocks_max * ng));
-    int* d_changed = reinterpret_cast<int*>(carve(64));
-    int32_t* d_total = d_changed + 4;
+    int32_t* d_total = reinterpret_cast<int32_t*>(carve(64));
+    int* d_changed = reinterpret_cast<int*>(carve(4 * kMaxScanIterations));  // one flag per round
 
     int64_t emitted = 0;
     int max_iter = 0;
@@ -490,26 +502,42 @@ int Ctx::consistency_scan(int mode, int n_views, const int32_t* src_off, const i
         launches += 2;
         bool converged = n_ngb == 0;
         int it = 0;
-        for (; !converged && it < kMaxScanIterations; ++it) {
-            k_accept<<<blocks, 256, 0, stream>>>(eff, wexp, n_ngb, dyn, acc, npix);
-            k_last_local<<<dim3(nblocks, n_ngb), kScanBlock, 0, stream>>>(eff, n_ngb, last, block_max, npix);
-            k_last_blocks<<<1, 32, 0, stream>>>(block_max, nblocks, n_ngb);
-            k_last_combine<<<blocks, 256, 0, stream>>>(last, block_max, n_ngb, npix, nblocks);
-            for (int j = 0; j < n_ngb; ++j) {
-                const ScanView& vs = hv[src_ids[src_off[i] + j]];
-                cudaMemsetAsync(vs.marktime, 0x7f, 4 * (size_t)vs.W * vs.H, stream);
-                if (mode == 0) cudaMemsetAsync(vs.marklast, 0xff, 4 * (size_t)vs.W * vs.H, stream);
+        int max_sp = 0;
+        for (int j = 0; j < n_ngb; ++j) {
+            const ScanView& vs = hv[src_ids[src_off[i] + j]];
+            max_sp = std::max(max_sp, vs.W * vs.H);
+        }
+        const dim3 reset_grid((max_sp + 255) / 256, std::max(1, n_ngb));
+        // rounds of the fixed point run kRoundsPerCheck at a time between reads of their change
+        // flags: a round after the one that changed nothing recomputes the same state from the same
+        // eff, so the extra rounds leave every result as it was at the fixed point
+        while (!converged && it < kMaxScanIterations) {
+            const int batch = std::min(kRoundsPerCheck, kMaxScanIterations - it);
+            cudaMemsetAsync(d_changed + it, 0, 4 * (size_t)batch, stream);
+            for (int r = 0; r < batch; ++r) {
+                k_accept<<<blocks, 256, 0, stream>>>(eff, wexp, n_ngb, dyn, acc, npix);
+                k_last_local<<<dim3(nblocks, n_ngb), kScanBlock, 0, stream>>>(eff, n_ngb, last, block_max, npix);
+                k_last_blocks<<<1, 32, 0, stream>>>(block_max, nblocks, n_ngb);
+                k_last_combine<<<blocks, 256, 0, stream>>>(last, block_max, n_ngb, npix, nblocks);
+                k_reset_marks<<<reset_grid, 256, 0, stream>>>(d_views, srcs, mode == 0 ? 1 : 0);
+                if (mode == 0) k_marks<0><<<blocks, 256, 0, stream>>>(d_views, srcs, n_ngb, pos, last, acc, npix);
+                else k_marks<1><<<blocks, 256, 0, stream>>>(d_views, srcs, n_ngb, pos, last, acc, npix);
+                k_update_eff<<<blocks, 256, 0, stream>>>(d_views, srcs, n_ngb, pos, test, eff, d_changed + it + r,
+                                                         npix, 1);
+                launches += 7;
             }
-            if (mode == 0) k_marks<0><<<blocks, 256, 0, stream>>>(d_views, srcs, n_ngb, pos, last, acc, npix);
-            else k_marks<1><<<blocks, 256, 0, stream>>>(d_views, srcs, n_ngb, pos, last, acc, npix);
-            cudaMemsetAsync(d_changed, 0, 4, stream);
-            k_update_eff<<<blocks, 256, 0, stream>>>(d_views, srcs, n_ngb, pos, test, eff, d_changed, npix, 1);
-            launches += 6;
-            int changed = 0;
-            e = cudaMemcpyAsync(&changed, d_changed, 4, cudaMemcpyDeviceToHost, stream);
+            int changed[kRoundsPerCheck];
+            e = cudaMemcpyAsync(changed, d_changed + it, 4 * (size_t)batch, cudaMemcpyDeviceToHost, stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
             if (e != cudaSuccess) return cuda_fail(e, "consistency iteration");
-            converged = changed == 0;
+            int r = 0;
+            while (r < batch && changed[r] != 0) ++r;
+            if (r < batch) {
+                converged = true;
+                it += r + 1;
+            } else {
+                it += batch;
+            }
         }
         if (!converged) {
             for (int j = 0; j < n_ngb; ++j) {
