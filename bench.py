@@ -401,7 +401,8 @@ def stage_breakdown(prof, step_ms: float, n_views: int, steps: int) -> dict:
     """Device seconds per reference view of each stage of a step (CUDA events around every stage)."""
     k = 1e-3 / max(steps, 1) / n_views
     sec = {"patchmatch_gpu": (prof.init_ms + prof.sweep_ms) * k, "confidence": prof.confidence_ms * k,
-           "prior": prof.prior_ms * k, "jbu": prof.jbu_ms * k, "fusion": prof.fusion_ms * k}
+           "prior": prof.prior_ms * k, "jbu": prof.jbu_ms * k, "fusion": prof.fusion_ms * k,
+           "level_images": prof.level_ms * k}
     sec["other"] = max(0.0, step_ms * 1e-3 / n_views - sum(sec.values()))
     return {"views": n_views, "seconds_per_view": {a: round(b, 5) for a, b in sec.items()}}
 

@@ -76,7 +76,7 @@ class Profile(ctypes.Structure):
                 ("init_view_evals", ctypes.c_uint64), ("sweep_view_evals", ctypes.c_uint64),
                 ("sweep_sampled", ctypes.c_uint64),
                 ("confidence_ms", ctypes.c_double), ("prior_ms", ctypes.c_double), ("jbu_ms", ctypes.c_double),
-                ("fusion_ms", ctypes.c_double)]
+                ("fusion_ms", ctypes.c_double), ("level_ms", ctypes.c_double)]
 
 
 class ReconOptions(ctypes.Structure):

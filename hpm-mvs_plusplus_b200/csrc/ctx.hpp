@@ -16,7 +16,7 @@ constexpr int kNumMaps = 16;
 
 // Kinds of the profiling events (hpm_profile): PatchMatch launches and the other stages of hpm_reconstruct.
 enum { HPM_STAGE_INIT = 0, HPM_STAGE_SWEEP = 1, HPM_STAGE_CONFIDENCE = 2, HPM_STAGE_PRIOR = 3, HPM_STAGE_JBU = 4,
-       HPM_STAGE_FUSION = 5 };
+       HPM_STAGE_FUSION = 5, HPM_STAGE_LEVEL = 6 };
 
 struct DevMap {
     float* ptr = nullptr;

@@ -214,7 +214,7 @@ int Ctx::reconstruct(int n_views, const hpm_camera* cams, const int32_t* src_off
             hpm_camera c = cams[i];
             const float sx = w / (float)v.orig_w, sy = h / (float)v.orig_h;
             c.K[0] *= sx; c.K[2] *= sx; c.K[4] *= sy; c.K[5] *= sy;
-            rc = prepare_level_image(i, w, h, c);
+            rc = timed(HPM_STAGE_LEVEL, [&]() { return prepare_level_image(i, w, h, c); });
             if (rc) return rc;
         }
         const int level = max_num_downscale;

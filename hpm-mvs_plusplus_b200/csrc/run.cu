@@ -317,6 +317,7 @@ int Ctx::profile_read(hpm_profile* out) {
         case HPM_STAGE_CONFIDENCE: out->confidence_ms += ms; break;
         case HPM_STAGE_PRIOR: out->prior_ms += ms; break;
         case HPM_STAGE_JBU: out->jbu_ms += ms; break;
+        case HPM_STAGE_LEVEL: out->level_ms += ms; break;
         default: out->fusion_ms += ms; break;
         }
     }

@@ -337,6 +337,7 @@ typedef struct hpm_profile {
     double prior_ms;           /*   prior construction (support points, raster, fits, reload; the host */
     double jbu_ms;             /*   Delaunay triangulations overlap it and are not included), JBU and */
     double fusion_ms;          /*   fusion */
+    double level_ms;           /* device time of the level images: resize, grey conversion, Canny */
 } hpm_profile;
 
 /* Turns profiling on (flags) or off (0).  Timing adds two event records per
