@@ -112,12 +112,15 @@ __global__ void k_canny_nms(const int* __restrict__ mag, const short2* __restric
 // Hysteresis: weak pixels 8-connected to a strong pixel become strong.  Each
 // block propagates inside its 32x8 tile (plus a one-pixel halo it reads) to a
 // fixed point; the host repeats the launch until no block changed anything.
+constexpr int kHystTile = 32;  // hysteresis tiles are 32 x 32 pixels, one thread each
+
 __global__ void k_canny_hyst(uint8_t* __restrict__ state, int W, int H, int* __restrict__ changed) {
-    __shared__ uint8_t t[10][34];
+    __shared__ uint8_t t[kHystTile + 2][kHystTile + 2];
     __shared__ int any;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8;
-    for (int k = threadIdx.y * 32 + threadIdx.x; k < 10 * 34; k += 256) {
-        const int ty = k / 34, tx = k % 34;
+    const int x0 = blockIdx.x * kHystTile, y0 = blockIdx.y * kHystTile;
+    for (int k = threadIdx.y * kHystTile + threadIdx.x; k < (kHystTile + 2) * (kHystTile + 2);
+         k += kHystTile * kHystTile) {
+        const int ty = k / (kHystTile + 2), tx = k % (kHystTile + 2);
         const int gx = x0 + tx - 1, gy = y0 + ty - 1;
         t[ty][tx] = (gx >= 0 && gx < W && gy >= 0 && gy < H) ? state[(size_t)gy * W + gx] : 0;
     }
@@ -125,7 +128,7 @@ __global__ void k_canny_hyst(uint8_t* __restrict__ state, int W, int H, int* __r
     const int lx = threadIdx.x + 1, ly = threadIdx.y + 1;
     const int gx = x0 + threadIdx.x, gy = y0 + threadIdx.y;
     bool mine = false;
-    for (int iter = 0; iter < 32 * 8; ++iter) {  // a tile path has at most 256 pixels
+    for (int iter = 0; iter < kHystTile * kHystTile; ++iter) {  // a path inside a tile has at most 1024 pixels
         if (threadIdx.x == 0 && threadIdx.y == 0) any = 0;
         __syncthreads();
         if (gx < W && gy < H && t[ly][lx] == 1) {
@@ -207,17 +210,30 @@ int Ctx::canny_view(int view) {
     k_canny_grad<<<g, b, 0, stream>>>(v.color, W, H, canny_mag, canny_grad);
     k_canny_nms<<<g, b, 0, stream>>>(canny_mag, canny_grad, W, H, 50, 150, canny_state);
     launches += 2;
-    int* d_changed = reinterpret_cast<int*>(canny_state + ((n + 3) & ~size_t(3)));
-    const int max_rounds = (int)(g.x * g.y) + 2;  // every round extends each path into a new tile
-    for (int r = 0; r < max_rounds; ++r) {
-        cudaMemsetAsync(d_changed, 0, 4, stream);
-        k_canny_hyst<<<g, dim3(32, 8), 0, stream>>>(canny_state, W, H, d_changed);
-        ++launches;
-        int changed = 0;
-        e = cudaMemcpyAsync(&changed, d_changed, 4, cudaMemcpyDeviceToHost, stream);
+    int* d_changed = reinterpret_cast<int*>(canny_state + ((n + 3) & ~size_t(3)));  // one flag per round
+    // A round grows every weak path to the end of its tile and one pixel into the next, so a path
+    // crossing k tiles takes k rounds; long weak chains (flat, noisy regions) take hundreds.  Rounds
+    // run kHystRounds at a time between host reads of their change flags: a round after one that
+    // changed nothing finds the same state and changes nothing, so the extra rounds leave the edge
+    // map as it was when the first of them had converged.
+    constexpr int kHystRounds = 8;
+    const dim3 hg((W + kHystTile - 1) / kHystTile, (H + kHystTile - 1) / kHystTile);
+    // every round before the last marks at least one weak pixel strong, so the loop ends by itself
+    // within (weak pixels + 1) rounds; n + 2 only bounds it
+    const int max_rounds = (int)std::min<size_t>(n + 2, 0x7fffffff);
+    for (int r0 = 0; r0 < max_rounds; r0 += kHystRounds) {
+        const int batch = std::min(kHystRounds, max_rounds - r0);
+        cudaMemsetAsync(d_changed, 0, 4 * (size_t)batch, stream);
+        for (int r = 0; r < batch; ++r)
+            k_canny_hyst<<<hg, dim3(kHystTile, kHystTile), 0, stream>>>(canny_state, W, H, d_changed + r);
+        launches += batch;
+        int changed[kHystRounds];
+        e = cudaMemcpyAsync(changed, d_changed, 4 * (size_t)batch, cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_fail(e, "canny hysteresis");
-        if (!changed) break;
+        bool done = false;
+        for (int r = 0; r < batch; ++r) done = done || !changed[r];
+        if (done) break;
     }
     k_canny_out<<<(int)((n + 255) / 256), 256, 0, stream>>>(canny_state, (int)n, v.canny);
     ++launches;

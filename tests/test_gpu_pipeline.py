@@ -50,6 +50,29 @@ def test_level_image_matches_cv2(ctx, size, target):
     assert np.array_equal(edges, cv2.Canny(ref, 50, 150))
 
 
+def test_canny_hysteresis_follows_a_long_weak_chain(ctx):
+    """A weak edge (Sobel L1 magnitude 80, between the thresholds 50 and 150) that winds across the
+    whole image as a serpentine, joined to strong edges only at its start: hysteresis must carry
+    the strong label along all of it, through hundreds of tile crossings, as cv2.Canny's flood
+    fill does."""
+    w, h = 1024, 768
+    img = np.full((h, w, 3), 100, np.uint8)
+    rows = list(range(20, h - 20, 38))
+    for k, y in enumerate(rows):
+        cv2.rectangle(img, (20, y), (w - 21, y + 4), (120, 120, 120), -1)
+        if k + 1 < len(rows):
+            x = w - 25 if k % 2 == 0 else 20
+            cv2.rectangle(img, (x, y), (x + 4, rows[k + 1] + 4), (120, 120, 120), -1)
+    cv2.rectangle(img, (14, 14), (30, 30), (230, 230, 230), -1)  # the strong start
+    ctx.set_image(7, img)
+    cam = hpm_b200.Camera.make(np.diag([w, w, 1.0]), np.eye(3), np.zeros(3), w, h, 1, 5)
+    ctx.prepare_level(7, w, h, cam)
+    _, _, edges = ctx.get_level(7)
+    ref = cv2.Canny(img, 50, 150)
+    assert (ref > 0).sum() > 20000  # the chain is kept, not only the start
+    assert np.array_equal(edges, ref)
+
+
 def _scene(w, h, seed=1):
     from hpm_b200 import synth
     return synth.make_scene(n_views=5, width=w, height=h, seed=seed, n_src=4)
