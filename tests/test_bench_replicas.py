@@ -61,3 +61,30 @@ def test_level_sizes_follow_the_reference_pyramid():
     # one 800x600 and one 1600x1200 level: photometric + 1 prior + 3 geometric runs, then
     # hierarchy + 2 prior + 3 geometric runs
     assert bench.view_pixel_runs(1600, 1200, 1) == 800 * 600 * 5 + 1600 * 1200 * 6
+
+
+def test_depth_accuracy_at_scaled_working_sizes():
+    """The accuracy the bench reports: maps at the truth's size are compared pixel by pixel; maps
+    smaller by an integer factor f (--initial-image-scale f) against truth pixel (f*x, f*y), the
+    pixel whose ray the scaled camera's pixel x looks along; other sizes give None."""
+    import numpy as np
+
+    bench = _bench()
+
+    class View:
+        pass
+
+    class Scene:
+        pass
+
+    v = View()
+    yy, xx = np.mgrid[0:96, 0:128].astype(np.float32)
+    v.depth = 10.0 + 0.05 * xx + 0.02 * yy
+    v.depth[:8] = 0.0  # no truth there
+    sc = Scene()
+    sc.views = [v]
+    assert bench.depth_accuracy([v.depth.copy()], sc) == 1.0
+    quarter = v.depth[::4, ::4].copy()
+    assert bench.depth_accuracy([quarter], sc) == 1.0
+    assert bench.depth_accuracy([quarter * 1.02], sc) == 0.0  # every depth 2 % off
+    assert bench.depth_accuracy([np.zeros((50, 60), np.float32)], sc) is None
